@@ -1,0 +1,382 @@
+#!/usr/bin/env python3
+"""Benchmark: bit-exact Goldilocks coset LDE on B200.
+
+Workload (one step): coset LDE of 128 columns x 2^22 Goldilocks words,
+uniform in [0, p), bit-reversed evaluations in, blowup 2 (two cosets of
+128 x 2^22 out, 8 GiB), bit-reversed output -- inverse NTT, coset shift by
+g = 7, forward NTT.  Inputs (4 GiB) and outputs are far larger than L2, so
+no flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+ours       the fused LDE (bc_lde_fused) through the C ABI; also reports the
+           plain composition (bc_lde_plain), per-step p50/p99, the dominant
+           kernel's roofline and a CPU baseline (oracle, host cores).
+reference  the reference's own CUDA kernels (native/ntt.cu, compiled for
+           sm_100a into oracle/_ref/libref_ntt.so) driven exactly as its
+           callers drive them: one inverse batch_ntt then one forward
+           batch_ntt per coset.
+One JSON line on stdout (rank 0).  For N > 1 (torchrun) every rank runs the
+same per-GPU workload (weak scaling, no collective on the data path); the
+time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "era-boojum-cuda_b200"))
+
+P = 0xFFFFFFFF00000001
+METRIC = "bit-exact Goldilocks LDE Melem/s: batched vs plain, % HBM roofline; p99 ms"
+LOG_N, COLS, LOG_BLOWUP = 22, 128, 1
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([x.strip() for x in out.split(",")])
+            except Exception:
+                return
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = sorted(float(s[0]) for s in self.samples)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[3 + i].lower() == "active"})
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": float(self.samples[0][1]), "reasons": reasons,
+                "samples": len(sm)}
+
+
+def dist_setup(gpus: int):
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return rank, world, local
+
+
+def barrier_max(value: float, world: int) -> float:
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], device="cuda", dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def make_inputs(seed: int):
+    """128 x 2^22 words uniform in [0, p) generated on the device (seeded)."""
+    import torch
+
+    n = 1 << LOG_N
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    x = torch.randint(-(2**63), 2**63 - 1, (COLS * n,), device="cuda", dtype=torch.int64, generator=g)
+    # words >= p as unsigned are the signed range [-(2^32 - 1), -1]: fold them into [0, p)
+    x = torch.where((x < 0) & (x >= -(2**32 - 1)), x + (2**32 - 1), x)
+    return x
+
+
+def time_steps(fn, steps: int, warmup: int, world: int, stream):
+    """W untimed steps, then K steps between barriers; returns (total ms max over ranks, per-step ms)."""
+    import torch
+
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+    evs[0].record(stream)
+    for i in range(steps):
+        fn()
+        evs[i + 1].record(stream)
+    torch.cuda.synchronize()
+    per = [evs[i].elapsed_time(evs[i + 1]) for i in range(steps)]
+    total = evs[0].elapsed_time(evs[-1])
+    barrier(world)
+    return barrier_max(total, world), per
+
+
+def pct(xs, q):
+    s = sorted(xs)
+    return s[min(len(s) - 1, int(round(q / 100.0 * (len(s) - 1))))]
+
+
+def cpu_baseline(threads: int, budget_s: float = 12.0):
+    """Oracle LDE (C restatement, all host threads) on a bounded sample of whole columns."""
+    import numpy as np
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    n = 1 << LOG_N
+    rng = np.random.default_rng(42)
+    cols = threads
+    x = rng.integers(0, P, size=cols * n, dtype=np.uint64)
+    t0 = time.perf_counter()
+    oracle.lde(x, LOG_N, cols, n, LOG_BLOWUP, threads=threads)
+    dt = time.perf_counter() - t0
+    reps = max(1, int(budget_s / max(dt, 1e-3)) - 1)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        oracle.lde(x, LOG_N, cols, n, LOG_BLOWUP, threads=threads)
+    dt = (time.perf_counter() - t0) / reps
+    out_elems = (1 << LOG_BLOWUP) * n * cols
+    return {"value": out_elems / dt / 1e6, "unit": "Melem/s", "cores": threads, "kind": "port",
+            "sample": f"{cols} of {COLS} columns (2^{LOG_N}, blowup {1 << LOG_BLOWUP}) x {reps} reps, "
+                      f"{dt:.2f} s each; oracle/gl_oracle.c, one column per thread"}
+
+
+def run_ours(args, rank, world):
+    import ctypes
+
+    import torch
+
+    import bc_ntt
+
+    n = 1 << LOG_N
+    B = 1 << LOG_BLOWUP
+    L = bc_ntt.lib()
+    bc_ntt.Context.create(12, 12)
+    stream = torch.cuda.current_stream()
+    s_handle = stream.cuda_stream
+    x = make_inputs(1234 + rank)
+    out = torch.empty(B * COLS * n, device="cuda", dtype=torch.int64)
+    xp, op = x.data_ptr(), out.data_ptr()
+
+    def fused():
+        rc = L.bc_lde_fused(xp, op, LOG_N, COLS, n, n, COLS * n, LOG_BLOWUP, s_handle)
+        assert rc == 0, rc
+
+    def plain():
+        rc = L.bc_lde_plain(xp, op, LOG_N, COLS, n, n, COLS * n, LOG_BLOWUP, s_handle)
+        assert rc == 0, rc
+
+    # result of one fused step for the bit-exactness spot check against the plain path
+    fused()
+    torch.cuda.synchronize()
+    ref_sum = out.clone()
+    plain()
+    torch.cuda.synchronize()
+    bit_exact_vs_plain = bool(torch.equal(ref_sum, out))
+    del ref_sum
+
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        total_ms, per = time_steps(fused, args.steps, args.warmup, world, stream)
+    plain_ms, plain_per = time_steps(plain, max(3, args.steps // 2), 1, world, stream)
+
+    out_elems = B * n * COLS
+    value = world * args.steps * out_elems / (total_ms / 1e3) / 1e6
+    ms_per_step = total_ms / args.steps
+
+    # dominant kernel: per-kernel durations from events recorded between the fused LDE's launches
+    nk = ctypes.c_uint32(0)
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(8)]
+    ev_handles = (ctypes.c_void_p * 8)(*[e.cuda_event if hasattr(e, "cuda_event") else 0 for e in evs])
+    kern_ms = None
+    for e in evs:
+        e.record(stream)  # materialise the events
+    torch.cuda.synchronize()
+    if all(ev_handles):
+        reps = 3
+        acc = None
+        for _ in range(reps):
+            rc = L.bc_lde_fused_profiled(xp, op, LOG_N, COLS, n, n, COLS * n, LOG_BLOWUP, s_handle,
+                                         ctypes.cast(ev_handles, ctypes.c_void_p), 8, ctypes.byref(nk))
+            assert rc == 0
+            torch.cuda.synchronize()
+            d = [evs[i].elapsed_time(evs[i + 1]) for i in range(nk.value)]
+            acc = d if acc is None else [a + b for a, b in zip(acc, d)]
+        kern_ms = [a / reps for a in acc]
+
+    peak, peak_kind = measured_peaks()
+    # algorithmic bytes per kernel of the 2-pass fused plan (A: read+write n; B: read n, write B n; C: read+write B n)
+    col_bytes = 8 * n * COLS
+    kernels = [("inverse low window (A)", 2 * col_bytes), ("top window, all cosets (B)", (1 + B) * col_bytes),
+               ("forward low window, all cosets (C)", 2 * B * col_bytes)]
+    roofline = None
+    if kern_ms and len(kern_ms) == len(kernels):
+        dom = max(range(len(kern_ms)), key=lambda i: kern_ms[i])
+        name, byts = kernels[dom]
+        achieved = byts / (kern_ms[dom] / 1e3) / 1e9
+        roofline = {"bound": "hbm", "kernel": name, "achieved": round(achieved, 1), "peak": peak,
+                    "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+                    "traffic": None, "kernel_ms": [round(v, 3) for v in kern_ms],
+                    "step_algorithmic_frac": round(8 * n * COLS * (1 + B) / (ms_per_step / 1e3) / 1e9 / peak, 4)}
+
+    # end to end through the C ABI with host buffers: pinned H2D, LDE, D2H every step
+    hx = torch.empty(COLS * n, dtype=torch.int64, pin_memory=True)
+    hx.copy_(x)
+    hout = torch.empty(B * COLS * n, dtype=torch.int64, pin_memory=True)
+    dx = torch.empty_like(x)
+
+    def e2e_step():
+        dx.copy_(hx, non_blocking=True)
+        rc = L.bc_lde_fused(dx.data_ptr(), op, LOG_N, COLS, n, n, COLS * n, LOG_BLOWUP, s_handle)
+        assert rc == 0
+        hout.copy_(out, non_blocking=True)
+
+    e2e_steps = max(2, min(args.steps, 5))
+    e2e_ms, _ = time_steps(e2e_step, e2e_steps, 1, world, stream)
+    e2e_value = world * e2e_steps * out_elems / (e2e_ms / 1e3) / 1e6
+
+    line = {
+        "metric": METRIC, "value": round(value, 1), "unit": "Melem/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u64 (Goldilocks)", "data": "synthetic",
+        "config": {"workload": f"coset LDE {COLS} cols x 2^{LOG_N}, blowup {B}, bit-reversed in/out",
+                   "log_n": LOG_N, "columns": COLS, "blowup": B, "path": "bc_lde_fused",
+                   "l2": "inputs 4 GiB and outputs 8 GiB, larger than L2; no flush", "parallelism": f"replicas x{world}"},
+        "p50_ms": round(pct(per, 50), 4), "p99_ms": round(pct(per, 99), 4),
+        "plain": {"value": round(world * len(plain_per) * out_elems / (plain_ms / 1e3) / 1e6, 1),
+                  "ms_per_step": round(plain_ms / len(plain_per), 4), "path": "bc_lde_plain",
+                  "bit_exact_vs_fused": bit_exact_vs_plain},
+        "roofline": roofline,
+        "clocks": clk.summary(),
+        "e2e": {"value": round(e2e_value, 1), "unit": "Melem/s", "h2d_bytes_per_step": 8 * COLS * n,
+                "d2h_bytes_per_step": 8 * B * COLS * n, "ms_per_step": round(e2e_ms / e2e_steps, 3),
+                "path": "pinned host -> bc_lde_fused -> pinned host, one stream"},
+        "gpu_launches": args.steps * (len(kern_ms) if kern_ms else 3),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(os.cpu_count() or 1)
+    return line
+
+
+def run_reference(args, rank, world):
+    import torch
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    if not os.path.exists(oracle.REF_LIB):
+        return {"impl": "reference", "unavailable": "oracle/_ref/libref_ntt.so not built (needs the reference sources)"}
+    n = 1 << LOG_N
+    B = 1 << LOG_BLOWUP
+    ref = oracle.RefKernels()
+    stream = torch.cuda.current_stream()
+    s = stream.cuda_stream
+    x = make_inputs(1234 + rank)
+    out = torch.empty(B * COLS * n, device="cuda", dtype=torch.int64)
+    coef = out[(B - 1) * COLS * n:]
+    xp, op, cp = x.data_ptr(), out.data_ptr(), coef.data_ptr()
+
+    def step(src=None):
+        ref.batch_ntt(src or xp, cp, LOG_N, COLS, n, n, True, True, 0, 0, s)
+        for k in range(B):
+            ref.batch_ntt(cp, op + 8 * k * COLS * n, LOG_N, COLS, n, n, False, False, LOG_BLOWUP, k, s)
+
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        total_ms, per = time_steps(step, args.steps, args.warmup, world, stream)
+    out_elems = B * n * COLS
+    value = world * args.steps * out_elems / (total_ms / 1e3) / 1e6
+    hx = torch.empty(COLS * n, dtype=torch.int64, pin_memory=True)
+    hx.copy_(x)
+    hout = torch.empty(B * COLS * n, dtype=torch.int64, pin_memory=True)
+    dx = torch.empty_like(x)
+
+    def e2e_step():
+        dx.copy_(hx, non_blocking=True)
+        step(dx.data_ptr())
+        hout.copy_(out, non_blocking=True)
+
+    e2e_steps = max(2, min(args.steps, 5))
+    e2e_ms, _ = time_steps(e2e_step, e2e_steps, 1, world, stream)
+    return {
+        "metric": METRIC, "value": round(value, 1), "unit": "Melem/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u64 (Goldilocks)", "data": "synthetic", "impl": "reference",
+        "reference_kind": ("the reference's own CUDA kernels (native/ntt.cu) compiled for sm_100a, driven like "
+                           "src/ntt.rs batch_ntt_internal: 1 inverse + 1 forward call per coset; the reference "
+                           "has no CPU implementation of this path (boojum's CPU NTT is not vendored)"),
+        "config": {"workload": f"coset LDE {COLS} cols x 2^{LOG_N}, blowup {B}, bit-reversed in/out",
+                   "log_n": LOG_N, "columns": COLS, "blowup": B, "path": "reference kernels",
+                   "l2": "inputs 4 GiB and outputs 8 GiB, larger than L2; no flush", "parallelism": f"replicas x{world}"},
+        "p50_ms": round(pct(per, 50), 4), "p99_ms": round(pct(per, 99), 4), "clocks": clk.summary(),
+        "e2e": {"value": round(world * e2e_steps * out_elems / (e2e_ms / 1e3) / 1e6, 1), "unit": "Melem/s",
+                "h2d_bytes_per_step": 8 * COLS * n, "d2h_bytes_per_step": 8 * B * COLS * n,
+                "ms_per_step": round(e2e_ms / e2e_steps, 3)},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    rank, world, _ = dist_setup(args.gpus)
+    line = run_ours(args, rank, world) if args.impl == "ours" else run_reference(args, rank, world)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,166 @@
+"""Python binding of libbc_ntt.so, mirroring the reference's Rust API.
+
+The reference exposes ``boojum_cuda::ntt::{batch_ntt_internal,
+batch_ntt_out_of_place, batch_ntt_in_place}`` (src/ntt.rs:179-369) and
+``boojum_cuda::context::Context::{create, destroy}`` (src/context.rs:171-296).
+This module exposes the same operations, with the same argument meaning, over
+the C ABI declared in include/bc_ntt.h.  Device buffers are torch CUDA tensors
+of dtype int64 or uint64 (the words are reinterpreted, never converted);
+streams default to torch's current stream.
+
+Argument violations raise ``ValueError`` (the reference panics on its
+asserts); CUDA failures raise ``RuntimeError``.  There is no CPU fallback:
+loading fails loudly when the shared library is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libbc_ntt.so")
+
+P = 0xFFFFFFFF00000001
+CUDA_ERROR_INVALID_VALUE = 1
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Load libbc_ntt.so (built in-tree by ``make -C era-boojum-cuda_b200``)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `make -C {_HERE}`")
+        L = ctypes.CDLL(LIB_PATH)
+        _declare(L)
+        _lib = L
+    return _lib
+
+
+_u32, _u64, _sz, _b, _vp = ctypes.c_uint32, ctypes.c_uint64, ctypes.c_size_t, ctypes.c_bool, ctypes.c_void_p
+
+# name -> argument types; every entry point returns cudaError_t (int).
+SIGNATURES = {
+    "bc_ntt_context_create": [_u32, _u32],
+    "bc_ntt_context_destroy": [],
+    "bc_batch_ntt_internal": [_vp, _vp, _u32, _u32, _u64, _u64, _b, _b, _u32, _u32, _vp],
+    "bc_batch_ntt_out_of_place": [_vp, _sz, _vp, _sz, _u32, _u32, _u64, _u64, _u64, _u64, _b, _b, _u32, _u32, _vp],
+    "bc_batch_ntt_in_place": [_vp, _sz, _u32, _u32, _u64, _u64, _b, _b, _u32, _u32, _vp],
+    "bc_batch_ntt_with_plan": [_vp, _vp, _u32, _u32, _u64, _u64, _b, _b, _u32, _u32, _vp, _vp, _u32, _vp],
+    "bc_lde_plain": [_vp, _vp, _u32, _u32, _u64, _u64, _u64, _u32, _vp],
+    "bc_lde_fused": [_vp, _vp, _u32, _u32, _u64, _u64, _u64, _u32, _vp],
+    "bc_lde_fused_profiled": [_vp, _vp, _u32, _u32, _u64, _u64, _u64, _u32, _vp, _vp, _u32, _vp],
+}
+
+
+def _declare(L):
+    for name, args in SIGNATURES.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = ctypes.c_int
+
+
+def _check(rc: int, what: str):
+    if rc == 0:
+        return
+    if rc == CUDA_ERROR_INVALID_VALUE:
+        raise ValueError(f"{what}: invalid argument (cudaErrorInvalidValue)")
+    raise RuntimeError(f"{what}: CUDA error {rc}")
+
+
+def _stream(stream):
+    if stream is None:
+        import torch
+
+        return torch.cuda.current_stream().cuda_stream
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream
+
+
+def _ptr(t, offset: int = 0):
+    return t.data_ptr() + 8 * offset
+
+
+def _len(t) -> int:
+    return t.numel()
+
+
+class Context:
+    """Twiddle/power tables on the current device (src/context.rs:157-297)."""
+
+    def __init__(self):
+        self.live = False
+
+    @classmethod
+    def create(cls, powers_of_w_coarse_log_count: int = 12, powers_of_g_coarse_log_count: int = 12) -> "Context":
+        _check(lib().bc_ntt_context_create(powers_of_w_coarse_log_count, powers_of_g_coarse_log_count),
+               "Context.create")
+        c = cls()
+        c.live = True
+        return c
+
+    def destroy(self):
+        if self.live:
+            _check(lib().bc_ntt_context_destroy(), "Context.destroy")
+            self.live = False
+
+
+def batch_ntt_internal(inputs_ptr: int, outputs_ptr: int, log_n: int, num_ntts: int,
+                       stride_between_input_arrays: int, stride_between_output_arrays: int,
+                       bitrev_inputs: bool, inverse: bool, log_extension_degree: int, coset_index: int,
+                       stream=None):
+    """Raw-pointer entry point (src/ntt.rs:179-191)."""
+    _check(lib().bc_batch_ntt_internal(inputs_ptr, outputs_ptr, log_n, num_ntts, stride_between_input_arrays,
+                                       stride_between_output_arrays, bitrev_inputs, inverse,
+                                       log_extension_degree, coset_index, _stream(stream)),
+           "batch_ntt_internal")
+
+
+def batch_ntt_out_of_place(inputs_matrix, outputs_matrix, log_n: int, num_ntts: int, inputs_offset: int,
+                           outputs_offset: int, stride_between_input_arrays: int,
+                           stride_between_output_arrays: int, bitrev_inputs: bool, inverse: bool,
+                           log_extension_degree: int, coset_index: int, stream=None):
+    """src/ntt.rs:294-335 over torch device tensors."""
+    _check(lib().bc_batch_ntt_out_of_place(_ptr(inputs_matrix), _len(inputs_matrix), _ptr(outputs_matrix),
+                                           _len(outputs_matrix), log_n, num_ntts, inputs_offset, outputs_offset,
+                                           stride_between_input_arrays, stride_between_output_arrays,
+                                           bitrev_inputs, inverse, log_extension_degree, coset_index,
+                                           _stream(stream)),
+           "batch_ntt_out_of_place")
+
+
+def batch_ntt_in_place(inputs_matrix, log_n: int, num_ntts: int, inputs_offset: int,
+                       stride_between_input_arrays: int, bitrev_inputs: bool, inverse: bool,
+                       log_extension_degree: int, coset_index: int, stream=None):
+    """src/ntt.rs:338-369 over a torch device tensor."""
+    _check(lib().bc_batch_ntt_in_place(_ptr(inputs_matrix), _len(inputs_matrix), log_n, num_ntts, inputs_offset,
+                                       stride_between_input_arrays, bitrev_inputs, inverse, log_extension_degree,
+                                       coset_index, _stream(stream)),
+           "batch_ntt_in_place")
+
+
+def batch_ntt_with_plan(inputs, outputs, log_n: int, num_ntts: int, stride_in: int, stride_out: int,
+                        bitrev_inputs: bool, inverse: bool, log_extension_degree: int, coset_index: int,
+                        plan, stream=None):
+    """Transform with an explicit pass plan: ``plan`` = [(bits, run), ...] from the top bits down."""
+    bits = (ctypes.c_uint8 * len(plan))(*[k for k, _ in plan])
+    runs = (ctypes.c_uint8 * len(plan))(*[c for _, c in plan])
+    _check(lib().bc_batch_ntt_with_plan(_ptr(inputs), _ptr(outputs), log_n, num_ntts, stride_in, stride_out,
+                                        bitrev_inputs, inverse, log_extension_degree, coset_index,
+                                        ctypes.cast(bits, _vp), ctypes.cast(runs, _vp), len(plan),
+                                        _stream(stream)),
+           "batch_ntt_with_plan")
+
+
+def lde(evals_bitrev, out, log_n: int, num_cols: int, log_blowup: int, stride_in: int | None = None,
+        stride_out: int | None = None, coset_stride: int | None = None, fused: bool = True, stream=None):
+    """Coset LDE of bit-reversed evaluations (torch device tensors); default layout coset-major."""
+    n = 1 << log_n
+    stride_in = n if stride_in is None else stride_in
+    stride_out = n if stride_out is None else stride_out
+    coset_stride = num_cols * stride_out if coset_stride is None else coset_stride
+    fn = lib().bc_lde_fused if fused else lib().bc_lde_plain
+    _check(fn(_ptr(evals_bitrev), _ptr(out), log_n, num_cols, stride_in, stride_out, coset_stride, log_blowup,
+              _stream(stream)), "lde")

@@ -1,0 +1,360 @@
+// lde.cu -- coset low-degree extension: plain composition and fused kernels.
+//
+// The reference ships no LDE function; its callers compose one inverse
+// transform with one forward transform per coset (src/ntt.rs:527-583 as used
+// by benches/ntt.rs:114-116):
+//     bit-reversed evaluations on H --iNTT b2n--> natural coefficients a_i
+//     --for k < B: n2b with (log_ext = log2 B, coset k)--> bit-reversed
+//     evaluations on c_k H, c_k = g * w_{nB}^k.
+// bc_lde_plain runs exactly that composition through bc_batch_ntt_internal.
+//
+// bc_lde_fused computes the same outputs with three kernels per plan:
+//   A  the inverse transform's passes below the top window (b2n, in -> T);
+//   B  one kernel on the top window: the inverse stages, the scale
+//      n^-1 * g^i, then for every coset the forward stages of that window;
+//   C  the forward passes below the top window for all cosets at once.
+// It rests on one identity: the B cosets together are the domain g * H_{Bn},
+// so the B forward transforms are the size-Bn transform of the zero-padded
+// sequence g^i a_i, and coset k is its output block brev(k).  Each coset's
+// forward transform is therefore the plain size-n transform of g^i a_i with
+// the index prefix brev(k) in its twiddles (column groups, ntt_pass.cuh):
+// the per-coset factors w_{nB}^{k i} vanish into the twiddles and the scale is
+// applied once per element instead of once per element and coset.  T is the
+// output block of the last coset, so no scratch memory is used.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "../../include/bc_ntt.h"
+#include "ntt_host.cuh"
+#include "ntt_pass.cuh"
+
+namespace bc {
+
+struct LdeTopParams {
+  const uint64_t *in; // T (or the evaluations when the plan has one pass)
+  uint64_t *out;      // coset block 0
+  uint64_t stride_in;
+  uint64_t stride_out;
+  uint64_t coset_stride;
+  uint32_t num_cols;
+  uint32_t log_n;
+  uint32_t lb; // = log_n - K
+  uint32_t log_blowup;
+  uint32_t log_g;
+  uint32_t cols_per_cta;
+  uint32_t canon_out; // single-pass plan: this kernel writes final values
+  uint32_t vec_in, vec_out;
+  DevTables tabs;
+};
+
+template <int K, int C>
+__global__ void __launch_bounds__(512) lde_top_kernel(const LdeTopParams p) {
+  constexpr int W = 1 << K;
+  using LastInv = RoundShape<K, true, true, (K + 3) / 4 - 1>; // last inverse round ...
+  using FirstFwd = RoundShape<K, false, false, 0>;            // ... holds the first forward round's groups
+  static_assert(LastInv::B == FirstFwd::B && LastInv::V == FirstFwd::V, "round hand-over mismatch");
+  constexpr int BB = FirstFwd::B, VV = FirstFwd::V, NV = 1 << VV, NG = 16 / NV;
+  extern __shared__ uint64_t smem[];
+  const uint32_t G = 1u << p.log_g;
+  const uint32_t TILE = G * W * C;
+  const uint32_t T = TILE / 16;
+  uint64_t *tile = smem;
+  uint64_t *tws_inv = smem + TILE + TILE / 16;
+  uint64_t *tws_fwd = tws_inv + (W - 1);
+  const uint32_t tid = threadIdx.x;
+
+  // top window: H = 0, the tile position is the run of low positions
+  const uint64_t base_off = (uint64_t)blockIdx.x << LogC<C>::v;
+  const uint32_t col_begin = blockIdx.y * p.cols_per_cta;
+  const uint32_t col_end = min(p.num_cols, col_begin + p.cols_per_cta);
+  fill_twiddles<K>(tws_inv, p.tabs, 1, 0, tid, T);
+
+  // scale n^-1 g^i of this thread's groups: i = base + lc + (w_j << lb), w_j = w | (j << BB)
+  const uint64_t g_step = g_power(p.tabs, 0, 1u << (p.lb + BB));
+  const uint64_t inv_n = p.tabs.inv_pow2[p.log_n];
+  const uint32_t nb = 1u << p.log_blowup;
+
+  for (uint32_t c0 = col_begin; c0 < col_end; c0 += G) {
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+      const uint32_t e = 2 * (tid + T * j);
+      uint32_t g;
+      uint64_t off;
+      tile_elem<K, C>(e, g, off, base_off, p.lb);
+      const uint32_t col = c0 + g;
+      uint64_t v0 = 0, v1 = 0;
+      if (col < col_end) {
+        const uint64_t *src = p.in + (uint64_t)col * p.stride_in + off;
+        if (p.vec_in) {
+          const ulonglong2 v = *reinterpret_cast<const ulonglong2 *>(src);
+          v0 = v.x;
+          v1 = v.y;
+        } else {
+          v0 = src[0];
+          v1 = src[1];
+        }
+      }
+      tile[pad16(e)] = v0;
+      tile[pad16(e) + 1] = v1;
+    }
+    __syncthreads();
+
+    // inverse stages of the window (bottom-up), all but the last round through shared memory
+    rounds_from<K, C, true, true, 0, (K + 3) / 4 - 1>(tile, tws_inv, tid, T);
+    uint64_t coef[16];
+    load_groups<K, C, BB, VV>(tile, coef, tid, T);
+    compute_groups<K, C, true, BB, VV>(coef, tws_inv, tid, T);
+#pragma unroll
+    for (int q = 0; q < NG; q++) {
+      uint32_t w;
+      const uint32_t gi = tid + T * q;
+      group_base<K, C, BB, VV>(gi, w);
+      const uint32_t i0 = (uint32_t)base_off + gi % C + (w << p.lb);
+      uint64_t s = gl::mul(inv_n, g_power(p.tabs, 0, i0));
+#pragma unroll
+      for (int j = 0; j < NV; j++) {
+        coef[q * NV + j] = gl::mul(coef[q * NV + j], s);
+        if (j + 1 < NV) s = gl::mul(s, g_step);
+      }
+    }
+
+    for (uint32_t k = 0; k < nb; k++) {
+      __syncthreads(); // previous coset's stores have read the tile and twiddles
+      fill_twiddles<K>(tws_fwd, p.tabs, 0, brev_bits(k, p.log_blowup), tid, T);
+      __syncthreads();
+      uint64_t x[16];
+#pragma unroll
+      for (int j = 0; j < 16; j++) x[j] = coef[j];
+      compute_groups<K, C, false, BB, VV>(x, tws_fwd, tid, T);
+      store_groups<K, C, BB, VV>(tile, x, tid, T);
+      __syncthreads();
+      rounds_from<K, C, false, false, 1>(tile, tws_fwd, tid, T);
+      uint64_t *out = p.out + (uint64_t)k * p.coset_stride;
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        const uint32_t e = 2 * (tid + T * j);
+        uint32_t g;
+        uint64_t off;
+        tile_elem<K, C>(e, g, off, base_off, p.lb);
+        const uint32_t col = c0 + g;
+        if (col >= col_end) continue;
+        uint64_t v0 = tile[pad16(e)], v1 = tile[pad16(e) + 1];
+        if (p.canon_out) {
+          v0 = gl::canon(v0);
+          v1 = gl::canon(v1);
+        }
+        uint64_t *dst = out + (uint64_t)col * p.stride_out + off;
+        if (p.vec_out) {
+          *reinterpret_cast<ulonglong2 *>(dst) = make_ulonglong2(v0, v1);
+        } else {
+          dst[0] = v0;
+          dst[1] = v1;
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+typedef void (*TopKernel)(const LdeTopParams);
+
+template <int K, int C> static TopKernel tk() { return lde_top_kernel<K, C>; }
+
+static TopKernel pick_top(int K, int C) {
+  if (C == 1) {
+    switch (K) {
+    case 1: return tk<1, 1>();
+    case 2: return tk<2, 1>();
+    case 3: return tk<3, 1>();
+    case 4: return tk<4, 1>();
+    case 5: return tk<5, 1>();
+    case 6: return tk<6, 1>();
+    case 7: return tk<7, 1>();
+    case 8: return tk<8, 1>();
+    case 9: return tk<9, 1>();
+    case 10: return tk<10, 1>();
+    case 11: return tk<11, 1>();
+    case 12: return tk<12, 1>();
+    default: return nullptr;
+    }
+  }
+  if (C == 8) {
+    switch (K) {
+    case 1: return tk<1, 8>();
+    case 2: return tk<2, 8>();
+    case 3: return tk<3, 8>();
+    case 4: return tk<4, 8>();
+    case 5: return tk<5, 8>();
+    case 6: return tk<6, 8>();
+    case 7: return tk<7, 8>();
+    case 8: return tk<8, 8>();
+    case 9: return tk<9, 8>();
+    default: return nullptr;
+    }
+  }
+  if (C == 4 && K == 10) return tk<10, 4>();
+  if (C == 2 && K == 11) return tk<11, 2>();
+  return nullptr;
+}
+
+static uint32_t ilog2_ceil(uint64_t x) {
+  uint32_t l = 0;
+  while ((1ull << l) < x) l++;
+  return l;
+}
+
+// Layout checks shared by both LDE paths: coset blocks and columns must be
+// disjoint windows, either coset-major (block k = cols x stride_out) or
+// column-major (each column holds its B cosets at coset_stride apart).
+bool lde_args_ok(uint32_t log_n, uint32_t num_cols, uint64_t stride_in, uint64_t stride_out, uint64_t coset_stride,
+                 uint32_t log_blowup) {
+  if (log_n < 1 || log_blowup < 1 || log_n + log_blowup > (uint32_t)TW_LOG) return false;
+  const uint64_t n = 1ull << log_n, B = 1ull << log_blowup;
+  if (stride_in < n || stride_out < n || coset_stride < n) return false;
+  if (num_cols == 0) return true;
+  const bool coset_major = coset_stride >= (uint64_t)(num_cols - 1) * stride_out + n;
+  const bool column_major = stride_out >= (B - 1) * coset_stride + n;
+  return coset_major || column_major;
+}
+
+// events (optional): ev[0] is recorded before the first kernel and ev[j + 1]
+// after kernel j, for as many events as are given.
+cudaError_t lde_fused(const Plan &pl, const uint64_t *in, uint64_t *out, uint32_t log_n, uint32_t num_cols,
+                      uint64_t stride_in, uint64_t stride_out, uint64_t coset_stride, uint32_t log_blowup,
+                      cudaStream_t stream, cudaEvent_t *ev = nullptr, uint32_t n_ev = 0) {
+  const DevTables *tabs = device_tables();
+  if (!tabs) return cudaErrorInitializationError;
+  if (num_cols == 0) return cudaSuccess;
+  uint32_t ev_used = 0;
+  auto mark = [&]() {
+    if (ev_used < n_ev) cudaEventRecord(ev[ev_used++], stream);
+  };
+  mark();
+  const uint32_t nb = 1u << log_blowup;
+  uint64_t *T = out + (uint64_t)(nb - 1) * coset_stride;
+  const int np = pl.npasses;
+  // A: inverse passes below the top window, bottom-up: in -> T
+  for (int s = 0; s < np - 1; s++) {
+    const int i = np - 1 - s;
+    PassLaunch q;
+    q.K = pl.pass[i].K;
+    q.C = pl.pass[i].C;
+    q.b2n = true;
+    q.in = s == 0 ? in : T;
+    q.out = T;
+    q.stride_in = s == 0 ? stride_in : stride_out;
+    q.stride_out = stride_out;
+    q.cols = num_cols;
+    q.log_n = log_n;
+    q.lb = plan_lb(pl, log_n, i);
+    q.inverse = true;
+    cudaError_t e = launch_pass(q, stream);
+    if (e != cudaSuccess) return e;
+    mark();
+  }
+  // B: top window
+  {
+    const int K = pl.pass[0].K, C = pl.pass[0].C;
+    LdeTopParams p{};
+    p.in = np == 1 ? in : T;
+    p.out = out;
+    p.stride_in = np == 1 ? stride_in : stride_out;
+    p.stride_out = stride_out;
+    p.coset_stride = coset_stride;
+    p.num_cols = num_cols;
+    p.log_n = log_n;
+    p.lb = log_n - K;
+    p.log_blowup = log_blowup;
+    const uint32_t wc_log = (uint32_t)K + ilog2_ceil((uint32_t)C);
+    p.log_g = choose_log_g(wc_log, num_cols);
+    const uint32_t G = 1u << p.log_g;
+    const uint64_t tiles = (1ull << log_n) >> wc_log;
+    const uint64_t chunks = (num_cols + G - 1) / G;
+    uint64_t factor = (tiles * chunks) / ((uint64_t)sm_count() * 8);
+    if (factor < 1) factor = 1;
+    if (factor > 8) factor = 8;
+    p.cols_per_cta = G * (uint32_t)factor;
+    p.canon_out = np == 1;
+    p.vec_in = ((uintptr_t)p.in % 16 == 0 && p.stride_in % 2 == 0) ? 1 : 0;
+    p.vec_out = ((uintptr_t)out % 16 == 0 && stride_out % 2 == 0 && coset_stride % 2 == 0) ? 1 : 0;
+    p.tabs = *tabs;
+    TopKernel kern = pick_top(K, C);
+    if (!kern) return cudaErrorInvalidValue;
+    const uint32_t tile = G << wc_log;
+    const size_t smem = ((size_t)tile + tile / 16 + 2 * ((1u << K) - 1)) * sizeof(uint64_t);
+    if (smem > 48 * 1024) {
+      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+    }
+    const uint64_t gy = (num_cols + p.cols_per_cta - 1) / p.cols_per_cta;
+    if (gy > 65535 || tiles > 0x7fffffffull) return cudaErrorInvalidConfiguration;
+    kern<<<dim3((uint32_t)tiles, (uint32_t)gy), tile / 16, smem, stream>>>(p);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    mark();
+  }
+  // C: forward passes below the top window for all cosets (column groups with prefix brev(k))
+  for (int i = 1; i < np; i++) {
+    PassLaunch q;
+    q.K = pl.pass[i].K;
+    q.C = pl.pass[i].C;
+    q.b2n = false;
+    q.in = out;
+    q.out = out;
+    q.stride_in = stride_out;
+    q.stride_out = stride_out;
+    q.group_stride_in = coset_stride;
+    q.group_stride_out = coset_stride;
+    q.cols = num_cols;
+    q.log_groups = log_blowup;
+    q.log_n = log_n;
+    q.lb = plan_lb(pl, log_n, i);
+    q.inverse = false;
+    q.canon_out = i == np - 1;
+    cudaError_t e = launch_pass(q, stream);
+    if (e != cudaSuccess) return e;
+    mark();
+  }
+  return cudaSuccess;
+}
+
+} // namespace bc
+
+using namespace bc;
+
+extern "C" cudaError_t bc_lde_plain(const uint64_t *evals_bitrev, uint64_t *out, uint32_t log_n, uint32_t num_cols,
+                                    uint64_t stride_in, uint64_t stride_out, uint64_t coset_stride,
+                                    uint32_t log_blowup, cudaStream_t stream) {
+  if (!lde_args_ok(log_n, num_cols, stride_in, stride_out, coset_stride, log_blowup)) return cudaErrorInvalidValue;
+  if (num_cols && (!evals_bitrev || !out)) return cudaErrorInvalidValue;
+  const uint32_t nb = 1u << log_blowup;
+  uint64_t *coef = out + (uint64_t)(nb - 1) * coset_stride;
+  cudaError_t e =
+      bc_batch_ntt_internal(evals_bitrev, coef, log_n, num_cols, stride_in, stride_out, true, true, 0, 0, stream);
+  for (uint32_t k = 0; e == cudaSuccess && k < nb; k++)
+    e = bc_batch_ntt_internal(coef, out + (uint64_t)k * coset_stride, log_n, num_cols, stride_out, stride_out, false,
+                              false, log_blowup, k, stream);
+  return e;
+}
+
+extern "C" cudaError_t bc_lde_fused(const uint64_t *evals_bitrev, uint64_t *out, uint32_t log_n, uint32_t num_cols,
+                                    uint64_t stride_in, uint64_t stride_out, uint64_t coset_stride,
+                                    uint32_t log_blowup, cudaStream_t stream) {
+  if (!lde_args_ok(log_n, num_cols, stride_in, stride_out, coset_stride, log_blowup)) return cudaErrorInvalidValue;
+  if (num_cols && (!evals_bitrev || !out)) return cudaErrorInvalidValue;
+  return lde_fused(default_plan(log_n), evals_bitrev, out, log_n, num_cols, stride_in, stride_out, coset_stride,
+                   log_blowup, stream);
+}
+
+extern "C" cudaError_t bc_lde_fused_profiled(const uint64_t *evals_bitrev, uint64_t *out, uint32_t log_n,
+                                             uint32_t num_cols, uint64_t stride_in, uint64_t stride_out,
+                                             uint64_t coset_stride, uint32_t log_blowup, cudaStream_t stream,
+                                             cudaEvent_t *events, uint32_t num_events, uint32_t *num_kernels) {
+  if (!lde_args_ok(log_n, num_cols, stride_in, stride_out, coset_stride, log_blowup)) return cudaErrorInvalidValue;
+  if (num_cols && (!evals_bitrev || !out)) return cudaErrorInvalidValue;
+  const Plan pl = default_plan(log_n);
+  if (num_kernels) *num_kernels = (uint32_t)(2 * pl.npasses - 1);
+  return lde_fused(pl, evals_bitrev, out, log_n, num_cols, stride_in, stride_out, coset_stride, log_blowup, stream,
+                   events, num_events);
+}

@@ -1,0 +1,66 @@
+// ntt_host.cuh -- host-side pieces shared by the NTT, LDE and batch code.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "tables.cuh"
+
+namespace bc {
+
+// A pass covers K index bits; C is the run of consecutive low positions a tile
+// spans (C = 1 only when the window starts at bit 0, where the tile is one
+// contiguous run of 2^K elements).
+struct PassCfg {
+  uint8_t K;
+  uint8_t C;
+};
+
+// Passes listed in natural->bit-reversed order: pass[0] owns the top bits,
+// pass[npasses-1] owns bits [0, K).  Bit-reversed->natural runs them in the
+// opposite order.
+struct Plan {
+  int npasses;
+  PassCfg pass[4];
+};
+
+// Per-device tables; returns nullptr when the context was not created on the
+// current device.
+const DevTables *device_tables();
+int current_device();
+int sm_count();
+
+Plan default_plan(uint32_t log_n);
+bool plan_valid(const Plan &pl, uint32_t log_n);
+
+// One pass over columns that may come in 2^log_groups groups (see ntt_pass.cuh).
+struct PassLaunch {
+  int K = 0, C = 1;
+  bool b2n = false;
+  const uint64_t *in = nullptr;
+  uint64_t *out = nullptr;
+  uint64_t stride_in = 0, stride_out = 0;
+  uint64_t group_stride_in = 0, group_stride_out = 0;
+  uint32_t cols = 0; // per group
+  uint32_t log_groups = 0;
+  uint32_t log_n = 0, lb = 0;
+  bool inverse = false, load_scale = false, store_scale = false, canon_out = false;
+  uint32_t has_coset = 0, coset_kshift = 0;
+};
+cudaError_t launch_pass(const PassLaunch &pl, cudaStream_t stream);
+
+// Window start (lowest bit) of pass i of a plan, passes listed top-down.
+uint32_t plan_lb(const Plan &pl, uint32_t log_n, int i);
+
+// Tile-size policy shared by the pass kernels: columns per tile iteration (log2).
+uint32_t choose_log_g(uint32_t wc_log, uint32_t cols);
+
+// Launches every pass of one batched transform; arguments already validated.
+cudaError_t launch_ntt(const Plan &pl, const uint64_t *in, uint64_t *out, uint32_t log_n, uint32_t num_ntts,
+                       uint64_t stride_in, uint64_t stride_out, bool bitrev_inputs, bool inverse, uint32_t log_ext,
+                       uint32_t coset_idx, cudaStream_t stream);
+
+// Argument checks of batch_ntt_internal (src/ntt.rs:192-200) with this
+// library's wider limits (log_n <= 27, log_n + log_extension_degree <= 30).
+bool ntt_args_ok(uint32_t log_n, uint64_t stride_in, uint64_t stride_out, uint32_t log_ext, uint32_t coset_idx);
+
+} // namespace bc

@@ -1,0 +1,47 @@
+// tables.cuh -- compact on-device twiddle and power tables (the "context").
+//
+// Replaces the reference's Context (src/context.rs:157-297) and its
+// __constant__ powers_data structs (native/context.cuh:11-48).  Instead of
+// process-global __constant__ symbols, every kernel receives a DevTables
+// struct by value, built once per device by bc_ntt_context_create.
+//
+// Roots of unity: w_{2^32} = 7^((p-1)/2^32), w_{2^k} = w_{2^32}^{2^(32-k)}.
+//
+// Twiddles.  A stage that pairs index bits at position a uses, for the pair
+// whose index has upper part r = idx >> (a + 1), the twiddle
+//     T[r] = w_{2^TW_LOG}^{brev_{TW_LOG-1}(r)}
+// (the reference's bit-reversed twiddle convention, native/ntt.cu:23-35:
+// T[r] does not depend on the stage or on log_n).  It is split in two levels,
+// r = rh * 2^TW_FINE + rl:
+//     T[r] = tw_lo[rl] * tw_hi[rh],
+//     tw_lo[rl] = w_{2^(TW_FINE+1)}^{brev_TW_FINE(rl)},
+//     tw_hi[rh] = w_{2^TW_LOG}^{brev_{TW_LOG-1-TW_FINE}(rh)}.
+// The inverse tables hold the same with w^-1.
+//
+// Powers for coset scaling: g = 7 and w_{2^PW_LOG}, two levels each:
+//     g^i   = g_lo[i & (2^G_FINE-1)] * g_hi[i >> G_FINE]      (i < 2^TW_LOG)
+//     w^e   = w_lo[e & (2^PW_FINE-1)] * w_hi[e >> PW_FINE]     (e < 2^PW_LOG)
+// with inverse variants for g^-i and w^-e.
+#pragma once
+#include <cstdint>
+
+namespace bc {
+
+constexpr int TW_LOG = 27;   // transform sizes up to 2^27 (regions r < 2^26)
+constexpr int TW_FINE = 13;  // tw_lo: 2^13 entries, tw_hi: 2^13 entries
+constexpr int G_FINE = 14;   // g_lo: 2^14, g_hi: 2^13  (i < 2^27)
+constexpr int PW_LOG = 30;   // LDE domains up to 2^30 (log_n + log_blowup <= 30)
+constexpr int PW_FINE = 15;  // w_lo: 2^15, w_hi: 2^15
+constexpr int MAX_LOG_N = TW_LOG;
+
+struct DevTables {
+  const uint64_t *tw_lo[2]; // [0] forward, [1] inverse
+  const uint64_t *tw_hi[2];
+  const uint64_t *g_lo[2];  // [0] g^i, [1] g^-i
+  const uint64_t *g_hi[2];
+  const uint64_t *w_lo[2];  // [0] w^e, [1] w^-e  with w = w_{2^PW_LOG}
+  const uint64_t *w_hi[2];
+  uint64_t inv_pow2[TW_LOG + 1]; // 2^-k
+};
+
+} // namespace bc

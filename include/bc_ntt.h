@@ -1,0 +1,123 @@
+/*
+ * bc_ntt.h -- C ABI of the B200 batched Goldilocks NTT / coset LDE library
+ * (era-boojum-cuda_b200/libbc_ntt.so).
+ *
+ * Field: Goldilocks, p = 2^64 - 2^32 + 1.  Elements are u64 words; inputs may
+ * be any u64 (non-canonical words are read mod p), outputs are canonical.
+ * Matrices are column-major: column j of a matrix starts at ptr + j * stride
+ * (u64 elements), exactly the layout of the reference's DeviceSlice matrices.
+ * Transform calls are asynchronous on the given stream and return a
+ * cudaError_t: argument violations that the reference rejects with
+ * assert!/panic (src/ntt.rs:192-200, 309-320, 351-352) return
+ * cudaErrorInvalidValue instead; launch failures return the CUDA error.
+ *
+ * Roots of unity are the generator-7 roots: w_{2^32} = 7^((p-1)/2^32) and
+ * w_{2^k} = w_{2^32}^{2^(32-k)}.  Limits: 1 <= log_n <= 27 and
+ * log_n + log_extension_degree <= 30 (the reference stops at 24,
+ * src/context.rs:12).
+ */
+#ifndef BC_NTT_H
+#define BC_NTT_H
+
+#include <cuda_runtime_api.h>
+#include <stdbool.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Replaces Context::create (src/context.rs:171-282).  Builds this library's
+ * twiddle and power tables on the CURRENT device (about 1.7 MB); every other
+ * call on that device requires it and returns cudaErrorInitializationError
+ * without it.  The two counts keep the reference's bounds check (<= 24); the
+ * table split itself is fixed.  Idempotent; thread-safe. */
+cudaError_t bc_ntt_context_create(uint32_t powers_of_w_coarse_log_count, uint32_t powers_of_g_coarse_log_count);
+
+/* Replaces Context::destroy (src/context.rs:284-296) for the current device. */
+cudaError_t bc_ntt_context_destroy(void);
+
+/* Replaces batch_ntt_internal (src/ntt.rs:179-191).
+ * num_ntts columns of n = 2^log_n elements.
+ *   bitrev_inputs = false: natural-order input, bit-reversed output
+ *   bitrev_inputs = true : bit-reversed input, natural-order output
+ *   inverse: inverse transform including the 1/n factor
+ *   log_extension_degree e, coset_index k: coset c = 7 * w_{n*2^e}^k (c = 1 when
+ *     e = 0); forward multiplies input i by c^i, inverse multiplies output i by
+ *     c^-i, i being the natural index.
+ * inputs == outputs (same strides) runs in place. */
+cudaError_t bc_batch_ntt_internal(const uint64_t *inputs, uint64_t *outputs, uint32_t log_n, uint32_t num_ntts,
+                                  uint64_t stride_between_input_arrays, uint64_t stride_between_output_arrays,
+                                  bool bitrev_inputs, bool inverse, uint32_t log_extension_degree,
+                                  uint32_t coset_index, cudaStream_t stream);
+
+/* Replaces batch_ntt_out_of_place (src/ntt.rs:294-335).  The *_len arguments
+ * are the element counts of the two device slices; the checks of
+ * src/ntt.rs:309-320 apply (offset + n <= stride, len >= num_ntts * stride,
+ * distinct buffers). */
+cudaError_t bc_batch_ntt_out_of_place(const uint64_t *inputs_matrix, size_t inputs_len, uint64_t *outputs_matrix,
+                                      size_t outputs_len, uint32_t log_n, uint32_t num_ntts, uint64_t inputs_offset,
+                                      uint64_t outputs_offset, uint64_t stride_between_input_arrays,
+                                      uint64_t stride_between_output_arrays, bool bitrev_inputs, bool inverse,
+                                      uint32_t log_extension_degree, uint32_t coset_index, cudaStream_t stream);
+
+/* Replaces batch_ntt_in_place (src/ntt.rs:338-369). */
+cudaError_t bc_batch_ntt_in_place(uint64_t *inputs_matrix, size_t len, uint32_t log_n, uint32_t num_ntts,
+                                  uint64_t inputs_offset, uint64_t stride_between_arrays, bool bitrev_inputs,
+                                  bool inverse, uint32_t log_extension_degree, uint32_t coset_index,
+                                  cudaStream_t stream);
+
+/* batch_ntt_internal with an explicit pass plan instead of the built-in one
+ * (the role of the reference's fixed PLANS table, src/ntt.rs:74-169, here
+ * chosen by the autotuner).  Pass i covers pass_bits[i] index bits, listed
+ * from the top bits down; pass_runs[i] is the run of consecutive low
+ * positions a tile spans (1 for the pass that owns bit 0; 8 for windows of
+ * <= 9 bits, 4 for 10, 2 for 11).  The bits must sum to log_n. */
+cudaError_t bc_batch_ntt_with_plan(const uint64_t *inputs, uint64_t *outputs, uint32_t log_n, uint32_t num_ntts,
+                                   uint64_t stride_in, uint64_t stride_out, bool bitrev_inputs, bool inverse,
+                                   uint32_t log_extension_degree, uint32_t coset_index, const uint8_t *pass_bits,
+                                   const uint8_t *pass_runs, uint32_t npasses, cudaStream_t stream);
+
+/* ---- coset low-degree extension ------------------------------------------
+ * Input: num_cols columns of n = 2^log_n bit-reversed evaluations on the
+ * subgroup H (column j at evals_bitrev + j * stride_in).  Output: for every
+ * coset k < B = 2^log_blowup the bit-reversed evaluations of the same
+ * polynomials on c_k H, c_k = 7 * w_{nB}^k, column j of coset k at
+ * out + k * coset_stride + j * stride_out.  Blocks and columns must be
+ * disjoint windows: coset-major (coset_stride >= (num_cols - 1) * stride_out
+ * + n) or column-major (stride_out >= (B - 1) * coset_stride + n).
+ * 1 <= log_blowup, log_n + log_blowup <= 27.  The input is not modified and
+ * must not overlap the output.  No memory is allocated: the output block of
+ * the last coset holds the intermediate values.
+ *
+ * The reference has no LDE function; these replace what its callers compose
+ * from batch_ntt_internal (src/ntt.rs:179-191): one inverse b2n call, then
+ * one forward n2b call per coset with (log_extension_degree = log_blowup,
+ * coset_index = k), as benches/ntt.rs:110-116 does. */
+
+/* The composition itself, one bc_batch_ntt_internal call per step. */
+cudaError_t bc_lde_plain(const uint64_t *evals_bitrev, uint64_t *out, uint32_t log_n, uint32_t num_cols,
+                         uint64_t stride_in, uint64_t stride_out, uint64_t coset_stride, uint32_t log_blowup,
+                         cudaStream_t stream);
+
+/* Same result from fused kernels: inverse passes, one kernel that ends the
+ * inverse transform, scales, and starts every coset's forward transform, then
+ * the remaining forward passes of all cosets together. */
+cudaError_t bc_lde_fused(const uint64_t *evals_bitrev, uint64_t *out, uint32_t log_n, uint32_t num_cols,
+                         uint64_t stride_in, uint64_t stride_out, uint64_t coset_stride, uint32_t log_blowup,
+                         cudaStream_t stream);
+
+/* bc_lde_fused that also records events[0] before its first kernel and
+ * events[j + 1] after kernel j (up to num_events events), for per-kernel
+ * timing; *num_kernels receives the number of kernels it launches. */
+cudaError_t bc_lde_fused_profiled(const uint64_t *evals_bitrev, uint64_t *out, uint32_t log_n, uint32_t num_cols,
+                                  uint64_t stride_in, uint64_t stride_out, uint64_t coset_stride,
+                                  uint32_t log_blowup, cudaStream_t stream, cudaEvent_t *events, uint32_t num_events,
+                                  uint32_t *num_kernels);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BC_NTT_H */

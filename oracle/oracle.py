@@ -1,0 +1,133 @@
+"""ctypes wrapper of the CPU oracle (liboracle.so) and of the compiled reference kernels.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+cpu_baseline / reference legs of bench.py -- never by the product library.
+
+* ``batch_ntt`` / ``lde``: CPU restatement (gl_oracle.c) of src/ntt.rs:179-369
+  semantics, numpy uint64 arrays in and out.
+* ``RefKernels``: the reference's own CUDA kernels (native/ntt.cu,
+  native/context.cu) built into oracle/_ref/libref_ntt.so by
+  ``make -C oracle ref``, driven by ref_glue.cu's restatement of
+  Context::create and batch_ntt_internal.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_LIB = os.path.join(HERE, "liboracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "libref_ntt.so")
+P = 0xFFFFFFFF00000001
+
+_u32, _u64, _i32, _vp = ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int, ctypes.c_void_p
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        L = ctypes.CDLL(ORACLE_LIB)
+        L.gl_oracle_batch_ntt.argtypes = [_vp, _vp, _u32, _u32, _u64, _u64, _i32, _i32, _u32, _u32, _i32]
+        L.gl_oracle_batch_ntt.restype = _i32
+        L.gl_oracle_lde.argtypes = [_vp, _vp, _u32, _u32, _u64, _u64, _u64, _u32, _i32]
+        L.gl_oracle_lde.restype = _i32
+        L.gl_oracle_dft_naive.argtypes = [_vp, _vp, _u32, _i32]
+        L.gl_oracle_dft_naive.restype = None
+        for f in ("gl_oracle_root_of_unity",):
+            getattr(L, f).argtypes = [_u32]
+            getattr(L, f).restype = _u64
+        L.gl_oracle_coset.argtypes = [_u32, _u32, _u32]
+        L.gl_oracle_coset.restype = _u64
+        L.gl_oracle_mul.argtypes = [_u64, _u64]
+        L.gl_oracle_mul.restype = _u64
+        L.gl_oracle_pow.argtypes = [_u64, _u64]
+        L.gl_oracle_pow.restype = _u64
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray):
+    assert a.dtype == np.uint64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_vp)
+
+
+def batch_ntt(inputs: np.ndarray, log_n: int, num_ntts: int, stride_in: int, stride_out: int,
+              bitrev_inputs: bool, inverse: bool, log_ext: int = 0, coset_idx: int = 0,
+              out: np.ndarray | None = None, threads: int = 1) -> np.ndarray:
+    """CPU batched NTT with batch_ntt_internal's argument meaning."""
+    if out is None:
+        out = np.zeros(max(num_ntts * stride_out, 1), dtype=np.uint64)
+    rc = lib().gl_oracle_batch_ntt(_p(inputs), _p(out), log_n, num_ntts, stride_in, stride_out,
+                                   int(bitrev_inputs), int(inverse), log_ext, coset_idx, threads)
+    if rc != 0:
+        raise ValueError("oracle: invalid arguments")
+    return out
+
+
+def lde(evals_bitrev: np.ndarray, log_n: int, num_cols: int, stride_in: int, log_blowup: int,
+        threads: int = 1) -> np.ndarray:
+    """Coset LDE (bit-reversed evaluations in; 2^log_blowup coset blocks of num_cols x n out, bit-reversed)."""
+    n = 1 << log_n
+    out = np.zeros((1 << log_blowup) * num_cols * n, dtype=np.uint64)
+    rc = lib().gl_oracle_lde(_p(evals_bitrev), _p(out), log_n, num_cols, stride_in, n, num_cols * n,
+                             log_blowup, threads)
+    if rc != 0:
+        raise ValueError("oracle: invalid arguments")
+    return out
+
+
+def dft_naive(x: np.ndarray, log_n: int, inverse: bool) -> np.ndarray:
+    y = np.zeros(1 << log_n, dtype=np.uint64)
+    lib().gl_oracle_dft_naive(_p(np.ascontiguousarray(x, dtype=np.uint64)), _p(y), log_n, int(inverse))
+    return y
+
+
+def root_of_unity(log_size: int) -> int:
+    return lib().gl_oracle_root_of_unity(log_size)
+
+
+def canon(a: np.ndarray) -> np.ndarray:
+    a = np.asarray(a, dtype=np.uint64)
+    return np.where(a >= np.uint64(P), a - np.uint64(P), a)
+
+
+def bitrev_permute(a: np.ndarray, log_n: int) -> np.ndarray:
+    """Bit-reverse the last axis (length 2^log_n)."""
+    idx = np.arange(1 << log_n, dtype=np.uint64)
+    rev = np.zeros_like(idx)
+    for b in range(log_n):
+        rev |= ((idx >> np.uint64(b)) & np.uint64(1)) << np.uint64(log_n - 1 - b)
+    return a[..., rev.astype(np.int64)]
+
+
+class RefKernels:
+    """The reference's own CUDA NTT kernels (needs a GPU and oracle/_ref/libref_ntt.so)."""
+
+    def __init__(self):
+        if not os.path.exists(REF_LIB):
+            raise RuntimeError(f"{REF_LIB} missing: `make -C oracle ref` where the reference sources exist")
+        L = ctypes.CDLL(REF_LIB)
+        L.ref_context_create.argtypes = [_u32, _u32]
+        L.ref_context_create.restype = _i32
+        L.ref_context_destroy.argtypes = []
+        L.ref_context_destroy.restype = _i32
+        L.ref_batch_ntt.argtypes = [_vp, _vp, _u32, _u32, _u32, _u32, ctypes.c_bool, ctypes.c_bool, _u32, _u32,
+                                    _vp]
+        L.ref_batch_ntt.restype = _i32
+        self.L = L
+        rc = L.ref_context_create(12, 12)
+        if rc != 0:
+            raise RuntimeError(f"ref_context_create failed: {rc}")
+
+    def batch_ntt(self, in_ptr: int, out_ptr: int, log_n: int, num_ntts: int, stride_in: int, stride_out: int,
+                  bitrev_inputs: bool, inverse: bool, log_ext: int, coset_idx: int, stream: int):
+        rc = self.L.ref_batch_ntt(in_ptr, out_ptr, log_n, num_ntts, stride_in, stride_out, bitrev_inputs, inverse,
+                                  log_ext, coset_idx, stream)
+        if rc != 0:
+            raise RuntimeError(f"ref_batch_ntt failed: {rc}")
+
+    def close(self):
+        self.L.ref_context_destroy()

@@ -1,0 +1,260 @@
+// ref_glue.cu -- host glue that runs the REFERENCE's own NTT kernels.
+//
+// TEST / BASELINE INFRASTRUCTURE ONLY (never linked into the product).
+// oracle/Makefile (target `ref`) compiles this file together with the
+// reference's native/ntt.cu and native/context.cu, as separate translation
+// units read from where they lie in the reference checkout (nothing is
+// copied), with relocatable device code, into oracle/_ref/libref_ntt.so.
+//
+// The reference's host side is Rust (src/context.rs, src/ntt.rs), which cannot
+// be built in this image (no Rust toolchain, boojum 0.2.2 not vendored), so
+// this file restates, in C++, exactly what that Rust does around the kernels:
+//   * ref_context_create   <- Context::create        src/context.rs:171-282
+//                             copy_to_symbols        src/context.rs:74-142
+//   * ref_batch_ntt        <- batch_ntt_internal     src/ntt.rs:179-290
+//                             (PLANS table           src/ntt.rs:74-169,
+//                              launch geometry       src/ntt.rs:257-270,
+//                              per-stage path        src/ntt.rs:203-241)
+// Roots of unity: boojum's domain_generator_for_size is replaced by the
+// generator-7 roots w_{2^k} = (7^((p-1)/2^32))^(2^(32-k)), the same choice the
+// C oracle (gl_oracle.c) and the product library make.
+
+#include "context.cuh"
+
+// The reference kernels (native/ntt_n2b.cuh, native/ntt_b2n.cuh), compiled in
+// their own translation unit; extern "C" linkage, signature of
+// native/ntt_n2b.cuh:104-108.
+#define REF_NTT_KERNEL(name)                                                                                           \
+  extern "C" __global__ void name(const base_field *, base_field *, const unsigned, const unsigned, const unsigned,   \
+                                  const unsigned, const unsigned, const bool, const unsigned, const unsigned,         \
+                                  const unsigned);
+REF_NTT_KERNEL(n2b_1_stage)
+REF_NTT_KERNEL(b2n_1_stage)
+REF_NTT_KERNEL(n2b_final_7_stages_warp)
+REF_NTT_KERNEL(n2b_final_8_stages_warp)
+REF_NTT_KERNEL(n2b_final_9_to_12_stages_block)
+REF_NTT_KERNEL(n2b_nonfinal_7_or_8_stages_block)
+REF_NTT_KERNEL(b2n_initial_7_stages_warp)
+REF_NTT_KERNEL(b2n_initial_8_stages_warp)
+REF_NTT_KERNEL(b2n_initial_9_to_12_stages_block)
+REF_NTT_KERNEL(b2n_noninitial_7_or_8_stages_block)
+#undef REF_NTT_KERNEL
+
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+namespace refglue {
+
+static constexpr uint64_t P = 0xffffffff00000001ull;
+typedef unsigned __int128 u128;
+
+static uint64_t mul(uint64_t a, uint64_t b) { return (uint64_t)(((u128)a * b) % P); }
+static uint64_t pw(uint64_t b, uint64_t e) {
+  uint64_t r = 1;
+  b %= P;
+  while (e) {
+    if (e & 1) r = mul(r, b);
+    b = mul(b, b);
+    e >>= 1;
+  }
+  return r;
+}
+static uint64_t inv(uint64_t a) { return pw(a, P - 2); }
+// domain_generator_for_size(2^k) restated with the generator-7 root choice.
+static uint64_t domain_generator(uint64_t size) {
+  unsigned k = 0;
+  while ((1ull << k) < size) k++;
+  return pw(pw(7, (P - 1) >> 32), 1ull << (32 - k));
+}
+static unsigned brev(unsigned x, unsigned bits) {
+  unsigned r = 0;
+  for (unsigned i = 0; i < bits; i++) r |= ((x >> i) & 1u) << (bits - 1 - i);
+  return r;
+}
+// generate_powers_dev (src/context.rs:144-155): distribute_powers from ONE,
+// then the optional bitreverse_enumeration_inplace over log2(len) bits.
+static cudaError_t upload_powers(uint64_t base, size_t len, bool bit_reverse, base_field **dst) {
+  std::vector<uint64_t> h(len);
+  uint64_t acc = 1;
+  for (size_t i = 0; i < len; i++) {
+    h[i] = acc;
+    acc = mul(acc, base);
+  }
+  if (bit_reverse) {
+    unsigned bits = 0;
+    while ((1ull << bits) < len) bits++;
+    std::vector<uint64_t> t(h);
+    for (size_t i = 0; i < len; i++) h[brev((unsigned)i, bits)] = t[i];
+  }
+  cudaError_t e = cudaMalloc(dst, len * sizeof(uint64_t));
+  if (e != cudaSuccess) return e;
+  return cudaMemcpy(*dst, h.data(), len * sizeof(uint64_t), cudaMemcpyHostToDevice);
+}
+
+static base_field *g_tables[10] = {};
+
+static powers_data make_pd(base_field *fine, unsigned fine_log, base_field *coarse, unsigned coarse_log) {
+  powers_data d;
+  d.fine.values = fine;
+  d.fine.mask = (1u << fine_log) - 1;
+  d.fine.log_count = fine_log;
+  d.coarse.values = coarse;
+  d.coarse.mask = (1u << coarse_log) - 1;
+  d.coarse.log_count = coarse_log;
+  return d;
+}
+
+} // namespace refglue
+
+using namespace refglue;
+
+extern "C" cudaError_t ref_context_destroy() {
+  for (auto &t : g_tables) {
+    if (t) cudaFree(t);
+    t = nullptr;
+  }
+  return cudaGetLastError();
+}
+
+extern "C" cudaError_t ref_context_create(unsigned w_coarse_log, unsigned g_coarse_log) {
+  if (w_coarse_log > OMEGA_LOG_ORDER || g_coarse_log > OMEGA_LOG_ORDER) return cudaErrorInvalidValue;
+  ref_context_destroy();
+  cudaError_t e;
+#define CK(x)                                                                                                          \
+  if ((e = (x)) != cudaSuccess) return e;
+  const uint64_t w24 = domain_generator(1ull << OMEGA_LOG_ORDER);
+  size_t len_fine = 1ull << (OMEGA_LOG_ORDER - w_coarse_log), len_coarse = 1ull << w_coarse_log;
+  CK(upload_powers(w24, len_fine, false, &g_tables[0]));                            // powers_of_w_fine
+  CK(upload_powers(domain_generator(len_coarse), len_coarse, false, &g_tables[1])); // powers_of_w_coarse
+  len_fine = 1ull << (OMEGA_LOG_ORDER - w_coarse_log - 1);
+  CK(upload_powers(w24, len_fine, true, &g_tables[2]));                                     // w fine bitrev
+  CK(upload_powers(domain_generator(len_coarse * 2), len_coarse, true, &g_tables[3]));      // w coarse bitrev
+  CK(upload_powers(inv(w24), len_fine, true, &g_tables[4]));                                // w inv fine bitrev
+  CK(upload_powers(inv(domain_generator(len_coarse * 2)), len_coarse, true, &g_tables[5])); // w inv coarse bitrev
+  len_fine = 1ull << (OMEGA_LOG_ORDER - g_coarse_log);
+  len_coarse = 1ull << g_coarse_log;
+  CK(upload_powers(7, len_fine, false, &g_tables[6]));               // g_f fine
+  CK(upload_powers(pw(7, len_fine), len_coarse, false, &g_tables[7])); // g_f coarse
+  const uint64_t g_inv = inv(7);
+  CK(upload_powers(g_inv, len_fine, false, &g_tables[8]));               // g_i fine
+  CK(upload_powers(pw(g_inv, len_fine), len_coarse, false, &g_tables[9])); // g_i coarse
+
+  // copy_to_symbols (src/context.rs:74-142), including its swapped fine/coarse
+  // log counts for powers_data_g_i (harmless when both splits are equal).
+  unsigned coarse_log = w_coarse_log, fine_log = OMEGA_LOG_ORDER - coarse_log;
+  powers_data d = make_pd(g_tables[0], fine_log, g_tables[1], coarse_log);
+  CK(cudaMemcpyToSymbol(powers_data_w, &d, sizeof(d)));
+  fine_log -= 1;
+  d = make_pd(g_tables[2], fine_log, g_tables[3], coarse_log);
+  CK(cudaMemcpyToSymbol(powers_data_w_bitrev_for_ntt, &d, sizeof(d)));
+  d = make_pd(g_tables[4], fine_log, g_tables[5], coarse_log);
+  CK(cudaMemcpyToSymbol(powers_data_w_inv_bitrev_for_ntt, &d, sizeof(d)));
+  coarse_log = g_coarse_log;
+  fine_log = OMEGA_LOG_ORDER - coarse_log;
+  d = make_pd(g_tables[6], fine_log, g_tables[7], coarse_log);
+  CK(cudaMemcpyToSymbol(powers_data_g_f, &d, sizeof(d)));
+  d = make_pd(g_tables[8], coarse_log, g_tables[9], fine_log);
+  CK(cudaMemcpyToSymbol(powers_data_g_i, &d, sizeof(d)));
+  uint64_t inv_sizes_host[OMEGA_LOG_ORDER + 1];
+  const uint64_t two_inv = inv(2);
+  uint64_t acc = 1;
+  for (unsigned i = 0; i <= OMEGA_LOG_ORDER; i++) {
+    inv_sizes_host[i] = acc;
+    acc = mul(acc, two_inv);
+  }
+  CK(cudaMemcpyToSymbol(inv_sizes, inv_sizes_host, sizeof(inv_sizes_host)));
+#undef CK
+  return cudaDeviceSynchronize();
+}
+
+namespace refglue {
+enum Kern { N2B_F7W, N2B_F8W, N2B_F912B, N2B_NF78B, B2N_I7W, B2N_I8W, B2N_I912B, B2N_NI78B, NONE };
+struct Step {
+  Kern k;
+  unsigned stages;
+};
+// PLANS, src/ntt.rs:74-169: [bitrev_inputs][log_n - 16][3]
+static const Step PLANS[2][9][3] = {
+    {{{N2B_NF78B, 8}, {N2B_F8W, 8}, {NONE, 0}},
+     {{N2B_NF78B, 8}, {N2B_F912B, 9}, {NONE, 0}},
+     {{N2B_NF78B, 8}, {N2B_F912B, 10}, {NONE, 0}},
+     {{N2B_NF78B, 8}, {N2B_F912B, 11}, {NONE, 0}},
+     {{N2B_NF78B, 8}, {N2B_F912B, 12}, {NONE, 0}},
+     {{N2B_NF78B, 7}, {N2B_NF78B, 7}, {N2B_F7W, 7}},
+     {{N2B_NF78B, 7}, {N2B_NF78B, 7}, {N2B_F8W, 8}},
+     {{N2B_NF78B, 7}, {N2B_NF78B, 8}, {N2B_F8W, 8}},
+     {{N2B_NF78B, 8}, {N2B_NF78B, 8}, {N2B_F8W, 8}}},
+    {{{B2N_I8W, 8}, {B2N_NI78B, 8}, {NONE, 0}},
+     {{B2N_I912B, 9}, {B2N_NI78B, 8}, {NONE, 0}},
+     {{B2N_I912B, 10}, {B2N_NI78B, 8}, {NONE, 0}},
+     {{B2N_I912B, 11}, {B2N_NI78B, 8}, {NONE, 0}},
+     {{B2N_I912B, 12}, {B2N_NI78B, 8}, {NONE, 0}},
+     {{B2N_I7W, 7}, {B2N_NI78B, 7}, {B2N_NI78B, 7}},
+     {{B2N_I8W, 8}, {B2N_NI78B, 7}, {B2N_NI78B, 7}},
+     {{B2N_I8W, 8}, {B2N_NI78B, 8}, {B2N_NI78B, 7}},
+     {{B2N_I8W, 8}, {B2N_NI78B, 8}, {B2N_NI78B, 8}}}};
+static const unsigned NTTS_PER_BLOCK_HOST = 8; // src/ntt.rs:174
+} // namespace refglue
+
+// batch_ntt_internal, src/ntt.rs:179-290.  Argument violations (asserts in the
+// Rust) return cudaErrorInvalidValue; launches are asynchronous on `stream`.
+extern "C" cudaError_t ref_batch_ntt(const uint64_t *inputs_ptr_in, uint64_t *outputs_ptr, unsigned log_n,
+                                     unsigned num_ntts, unsigned stride_in, unsigned stride_out, bool bitrev_inputs,
+                                     bool inverse, unsigned log_ext, unsigned coset_index, cudaStream_t stream) {
+  if (log_n < 1 || log_n + log_ext > OMEGA_LOG_ORDER) return cudaErrorInvalidValue;
+  const unsigned n = 1u << log_n;
+  if (n > stride_in || n > stride_out) return cudaErrorInvalidValue;
+  if (coset_index > 0 && (log_ext == 0 || coset_index >= (1u << log_ext))) return cudaErrorInvalidValue;
+  if (num_ntts == 0) return cudaSuccess;
+  const base_field *in0 = reinterpret_cast<const base_field *>(inputs_ptr_in);
+  base_field *out = reinterpret_cast<base_field *>(outputs_ptr);
+  if (log_n < 16) {
+    const unsigned threads = 128;
+    const unsigned blocks_per_ntt = (n + 2 * threads - 1) / (2 * threads);
+    const unsigned blocks = blocks_per_ntt * num_ntts;
+    for (unsigned stage = 0; stage < log_n; stage++) {
+      const base_field *in = stage == 0 ? in0 : out;
+      const unsigned sin = stage == 0 ? stride_in : stride_out;
+      if (bitrev_inputs)
+        b2n_1_stage<<<blocks, threads, 0, stream>>>(in, out, sin, stride_out, stage, 1, log_n, inverse,
+                                                         blocks_per_ntt, log_ext, coset_index);
+      else
+        n2b_1_stage<<<blocks, threads, 0, stream>>>(in, out, sin, stride_out, stage, 1, log_n, inverse,
+                                                         blocks_per_ntt, log_ext, coset_index);
+      cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+  }
+  const Step *plan = PLANS[bitrev_inputs ? 1 : 0][log_n - 16];
+  unsigned stage = 0;
+  const unsigned num_chunks = (num_ntts + NTTS_PER_BLOCK_HOST - 1) / NTTS_PER_BLOCK_HOST;
+  for (int i = 0; i < 3; i++) {
+    const Step st = plan[i];
+    if (st.k == NONE) continue;
+    const unsigned start_stage = stage;
+    const base_field *in = stage == 0 ? in0 : out;
+    const unsigned sin = stage == 0 ? stride_in : stride_out;
+    stage += st.stages;
+    dim3 block, grid;
+    void (*fn)(const base_field *, base_field *, unsigned, unsigned, unsigned, unsigned, unsigned, bool, unsigned,
+               unsigned, unsigned) = nullptr;
+    switch (st.k) {
+    case N2B_F7W: fn = n2b_final_7_stages_warp; grid = dim3(n / (4 * 128), num_chunks); block = 128; break;
+    case N2B_F8W: fn = n2b_final_8_stages_warp; grid = dim3(n / (4 * 256), num_chunks); block = 128; break;
+    case N2B_F912B: fn = n2b_final_9_to_12_stages_block; grid = dim3(n / 4096, num_chunks); block = 512; break;
+    case N2B_NF78B: fn = n2b_nonfinal_7_or_8_stages_block; grid = dim3(n / 4096, num_chunks); block = 512; break;
+    case B2N_I7W: fn = b2n_initial_7_stages_warp; grid = dim3(n / (4 * 128), num_chunks); block = 128; break;
+    case B2N_I8W: fn = b2n_initial_8_stages_warp; grid = dim3(n / (4 * 256), num_chunks); block = 128; break;
+    case B2N_I912B: fn = b2n_initial_9_to_12_stages_block; grid = dim3(n / 4096, num_chunks); block = 512; break;
+    case B2N_NI78B: fn = b2n_noninitial_7_or_8_stages_block; grid = dim3(n / 4096, num_chunks); block = 512; break;
+    default: return cudaErrorInvalidValue;
+    }
+    fn<<<grid, block, 0, stream>>>(in, out, sin, stride_out, start_stage, st.stages, log_n, inverse, num_ntts, log_ext,
+                                   coset_index);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return stage == log_n ? cudaSuccess : cudaErrorUnknown;
+}
