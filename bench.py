@@ -25,7 +25,6 @@ from __future__ import annotations
 import argparse
 import json
 import os
-import subprocess
 import sys
 import threading
 import time
@@ -48,32 +47,47 @@ def measured_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle samples during the timed region."""
+    """SM clock / throttle-reason samples during the timed region, read in-process through NVML.
+
+    (A polling nvidia-smi subprocess was seen to stall the GPU for hundreds of ms.)"""
+
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+               "sw_power_cap": 0x4}
 
     def __init__(self, index: int):
         self.index = index
         self.samples = []
         self._stop = threading.Event()
         self._t = None
+        self.error = None
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM))
+        except Exception as e:  # no NVML: report it instead of clocks
+            self.nv = None
+            self.error = str(e)
 
     def _run(self):
-        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
-             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-             "clocks_event_reasons.sw_power_cap")
+        nv = self.nv
         while not self._stop.is_set():
             try:
-                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
-                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
-                                     timeout=5).stdout.strip()
-                if out:
-                    self.samples.append([x.strip() for x in out.split(",")])
-            except Exception:
+                sm = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h) if hasattr(
+                    nv, "nvmlDeviceGetCurrentClocksEventReasons") else nv.nvmlDeviceGetCurrentClocksThrottleReasons(self.h)
+                self.samples.append((float(sm), int(r)))
+            except Exception as e:
+                self.error = str(e)
                 return
-            self._stop.wait(0.2)
+            self._stop.wait(0.05)
 
     def __enter__(self):
-        self._t = threading.Thread(target=self._run, daemon=True)
-        self._t.start()
+        if self.nv is not None:
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
         return self
 
     def __exit__(self, *a):
@@ -83,12 +97,11 @@ class ClockSampler:
 
     def summary(self):
         if not self.samples:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        sm = sorted(float(s[0]) for s in self.samples)
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[3 + i].lower() == "active"})
-        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": float(self.samples[0][1]), "reasons": reasons,
-                "samples": len(sm)}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [f"no samples: {self.error}"]}
+        sm = sorted(s for s, _ in self.samples)
+        reasons = sorted({k for _, r in self.samples for k, bit in self.REASONS.items() if r & bit})
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": self.max_mhz, "reasons": reasons, "samples": len(sm),
+                "source": "NVML"}
 
 
 def dist_setup(gpus: int):
@@ -205,7 +218,7 @@ def run_ours(args, rank, world):
     out = torch.empty(B * COLS * n, device="cuda", dtype=torch.int64)
     xp, op = x.data_ptr(), out.data_ptr()
 
-    def fused():
+    def fused():  # noqa: E306
         rc = L.bc_lde_fused(xp, op, LOG_N, COLS, n, n, COLS * n, LOG_BLOWUP, s_handle)
         assert rc == 0, rc
 
@@ -233,11 +246,11 @@ def run_ours(args, rank, world):
     # dominant kernel: per-kernel durations from events recorded between the fused LDE's launches
     nk = ctypes.c_uint32(0)
     evs = [torch.cuda.Event(enable_timing=True) for _ in range(8)]
-    ev_handles = (ctypes.c_void_p * 8)(*[e.cuda_event if hasattr(e, "cuda_event") else 0 for e in evs])
     kern_ms = None
     for e in evs:
-        e.record(stream)  # materialise the events
+        e.record(stream)  # torch creates the CUDA event on first record
     torch.cuda.synchronize()
+    ev_handles = (ctypes.c_void_p * 8)(*[e.cuda_event for e in evs])
     if all(ev_handles):
         reps = 3
         acc = None
@@ -251,10 +264,15 @@ def run_ours(args, rank, world):
         kern_ms = [a / reps for a in acc]
 
     peak, peak_kind = measured_peaks()
-    # algorithmic bytes per kernel of the 2-pass fused plan (A: read+write n; B: read n, write B n; C: read+write B n)
+    # bytes each kernel of the fused plan must move: inverse passes below the top window read+write the
+    # columns; the top-window kernel reads them once and writes every coset; the forward passes below the
+    # top window read+write every coset
     col_bytes = 8 * n * COLS
-    kernels = [("inverse low window (A)", 2 * col_bytes), ("top window, all cosets (B)", (1 + B) * col_bytes),
-               ("forward low window, all cosets (C)", 2 * B * col_bytes)]
+    npass = (nk.value + 1) // 2 if nk.value else 1
+    kernels = ([(f"lde inverse pass {i} (b2n)", 2 * col_bytes) for i in range(npass - 1)]
+               + [("lde_top_kernel (inverse top window, scale, forward top window, all cosets)",
+                   (1 + B) * col_bytes)]
+               + [(f"lde forward pass {i} (n2b, all cosets)", 2 * B * col_bytes) for i in range(npass - 1)])
     roofline = None
     if kern_ms and len(kern_ms) == len(kernels):
         dom = max(range(len(kern_ms)), key=lambda i: kern_ms[i])
@@ -367,7 +385,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--log-n", type=int, default=22, help="column length 2^log_n (default 22)")
+    ap.add_argument("--cols", type=int, default=128, help="columns (default 128)")
+    ap.add_argument("--log-blowup", type=int, default=1, help="log2 of the blowup (default 1)")
     args = ap.parse_args()
+    global LOG_N, COLS, LOG_BLOWUP
+    LOG_N, COLS, LOG_BLOWUP = args.log_n, args.cols, args.log_blowup
     rank, world, _ = dist_setup(args.gpus)
     line = run_ours(args, rank, world) if args.impl == "ours" else run_reference(args, rank, world)
     if rank == 0:
