@@ -51,7 +51,19 @@ SIGNATURES = {
     "bc_lde_plain": [_vp, _vp, _u32, _u32, _u64, _u64, _u64, _u32, _vp],
     "bc_lde_fused": [_vp, _vp, _u32, _u32, _u64, _u64, _u64, _u32, _vp],
     "bc_lde_fused_profiled": [_vp, _vp, _u32, _u32, _u64, _u64, _u64, _u32, _vp, _vp, _u32, _vp],
+    "bc_lde_batch_plan_create": [_vp, _u32, _vp],
+    "bc_lde_batch_run": [_vp, _vp],
+    "bc_lde_batch_status": [_vp, _vp, _vp],
+    "bc_lde_batch_plan_info": [_vp, _vp, _vp, _vp],
+    "bc_lde_batch_plan_destroy": [_vp],
 }
+
+
+class LdeJob(ctypes.Structure):
+    """bc_lde_job of include/bc_ntt.h."""
+    _fields_ = [("evals_bitrev", _vp), ("out", _vp), ("stride_in", _u64), ("stride_out", _u64),
+                ("coset_stride", _u64), ("log_n", _u32), ("num_cols", _u32), ("log_blowup", _u32),
+                ("reserved", _u32)]
 
 
 def _declare(L):
@@ -164,3 +176,48 @@ def lde(evals_bitrev, out, log_n: int, num_cols: int, log_blowup: int, stride_in
     fn = lib().bc_lde_fused if fused else lib().bc_lde_plain
     _check(fn(_ptr(evals_bitrev), _ptr(out), log_n, num_cols, stride_in, stride_out, coset_stride, log_blowup,
               _stream(stream)), "lde")
+
+
+class LdeBatch:
+    """A persistent-kernel batch plan over uneven LDE jobs (bc_lde_batch_*)."""
+
+    def __init__(self, jobs):
+        """jobs: list of (evals tensor, out tensor, log_n, num_cols, log_blowup) with dense coset-major outputs,
+        or LdeJob structures."""
+        arr = (LdeJob * max(1, len(jobs)))()
+        for i, j in enumerate(jobs):
+            if isinstance(j, LdeJob):
+                arr[i] = j
+            else:
+                ev, out, log_n, cols, log_b = j
+                n = 1 << log_n
+                arr[i] = LdeJob(_ptr(ev), _ptr(out), n, n, cols * n, log_n, cols, log_b, 0)
+        self._jobs = arr
+        self.handle = ctypes.c_void_p()
+        _check(lib().bc_lde_batch_plan_create(ctypes.cast(arr, _vp), len(jobs), ctypes.byref(self.handle)),
+               "bc_lde_batch_plan_create")
+
+    def run(self, stream=None):
+        _check(lib().bc_lde_batch_run(self.handle, _stream(stream)), "bc_lde_batch_run")
+
+    def status(self, stream=None) -> int:
+        st = ctypes.c_uint32(0)
+        _check(lib().bc_lde_batch_status(self.handle, _stream(stream), ctypes.byref(st)), "bc_lde_batch_status")
+        return st.value
+
+    def info(self):
+        r, i, g = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+        _check(lib().bc_lde_batch_plan_info(self.handle, ctypes.byref(r), ctypes.byref(i), ctypes.byref(g)),
+               "bc_lde_batch_plan_info")
+        return {"records": r.value, "items": i.value, "grid": g.value}
+
+    def close(self):
+        if self.handle:
+            _check(lib().bc_lde_batch_plan_destroy(self.handle), "bc_lde_batch_plan_destroy")
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

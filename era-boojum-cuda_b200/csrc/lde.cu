@@ -26,138 +26,18 @@
 #include <cstdint>
 
 #include "../../include/bc_ntt.h"
-#include "ntt_host.cuh"
-#include "ntt_pass.cuh"
+#include "lde.cuh"
 
 namespace bc {
 
-struct LdeTopParams {
-  const uint64_t *in; // T (or the evaluations when the plan has one pass)
-  uint64_t *out;      // coset block 0
-  uint64_t stride_in;
-  uint64_t stride_out;
-  uint64_t coset_stride;
-  uint32_t num_cols;
-  uint32_t log_n;
-  uint32_t lb; // = log_n - K
-  uint32_t log_blowup;
-  uint32_t log_g;
-  uint32_t cols_per_cta;
-  uint32_t canon_out; // single-pass plan: this kernel writes final values
-  uint32_t vec_in, vec_out;
-  DevTables tabs;
-};
-
 template <int K, int C>
-__global__ void __launch_bounds__(512) lde_top_kernel(const LdeTopParams p) {
-  constexpr int W = 1 << K;
-  using LastInv = RoundShape<K, true, true, (K + 3) / 4 - 1>; // last inverse round ...
-  using FirstFwd = RoundShape<K, false, false, 0>;            // ... holds the first forward round's groups
-  static_assert(LastInv::B == FirstFwd::B && LastInv::V == FirstFwd::V, "round hand-over mismatch");
-  constexpr int BB = FirstFwd::B, VV = FirstFwd::V, NV = 1 << VV, NG = 16 / NV;
+__global__ void __launch_bounds__(256, 2) lde_top_kernel(const LdeTopParams p) {
   extern __shared__ uint64_t smem[];
-  const uint32_t G = 1u << p.log_g;
-  const uint32_t TILE = G * W * C;
-  const uint32_t T = TILE / 16;
-  uint64_t *tile = smem;
-  uint64_t *tws_inv = smem + TILE + TILE / 16;
-  uint64_t *tws_fwd = tws_inv + (W - 1);
-  const uint32_t tid = threadIdx.x;
-
-  // top window: H = 0, the tile position is the run of low positions
-  const uint64_t base_off = (uint64_t)blockIdx.x << LogC<C>::v;
-  const uint32_t col_begin = blockIdx.y * p.cols_per_cta;
-  const uint32_t col_end = min(p.num_cols, col_begin + p.cols_per_cta);
-  fill_twiddles<K>(tws_inv, p.tabs, 1, 0, tid, T);
-
-  // scale n^-1 g^i of this thread's groups: i = base + lc + (w_j << lb), w_j = w | (j << BB)
-  const uint64_t g_step = g_power(p.tabs, 0, 1u << (p.lb + BB));
-  const uint64_t inv_n = p.tabs.inv_pow2[p.log_n];
-  const uint32_t nb = 1u << p.log_blowup;
-
-  for (uint32_t c0 = col_begin; c0 < col_end; c0 += G) {
-#pragma unroll
-    for (int j = 0; j < 8; j++) {
-      const uint32_t e = 2 * (tid + T * j);
-      uint32_t g;
-      uint64_t off;
-      tile_elem<K, C>(e, g, off, base_off, p.lb);
-      const uint32_t col = c0 + g;
-      uint64_t v0 = 0, v1 = 0;
-      if (col < col_end) {
-        const uint64_t *src = p.in + (uint64_t)col * p.stride_in + off;
-        if (p.vec_in) {
-          const ulonglong2 v = *reinterpret_cast<const ulonglong2 *>(src);
-          v0 = v.x;
-          v1 = v.y;
-        } else {
-          v0 = src[0];
-          v1 = src[1];
-        }
-      }
-      tile[pad16(e)] = v0;
-      tile[pad16(e) + 1] = v1;
-    }
-    __syncthreads();
-
-    // inverse stages of the window (bottom-up), all but the last round through shared memory
-    rounds_from<K, C, true, true, 0, (K + 3) / 4 - 1>(tile, tws_inv, tid, T);
-    uint64_t coef[16];
-    load_groups<K, C, BB, VV>(tile, coef, tid, T);
-    compute_groups<K, C, true, BB, VV>(coef, tws_inv, tid, T);
-#pragma unroll
-    for (int q = 0; q < NG; q++) {
-      uint32_t w;
-      const uint32_t gi = tid + T * q;
-      group_base<K, C, BB, VV>(gi, w);
-      const uint32_t i0 = (uint32_t)base_off + gi % C + (w << p.lb);
-      uint64_t s = gl::mul(inv_n, g_power(p.tabs, 0, i0));
-#pragma unroll
-      for (int j = 0; j < NV; j++) {
-        coef[q * NV + j] = gl::mul(coef[q * NV + j], s);
-        if (j + 1 < NV) s = gl::mul(s, g_step);
-      }
-    }
-
-    for (uint32_t k = 0; k < nb; k++) {
-      __syncthreads(); // previous coset's stores have read the tile and twiddles
-      fill_twiddles<K>(tws_fwd, p.tabs, 0, brev_bits(k, p.log_blowup), tid, T);
-      __syncthreads();
-      uint64_t x[16];
-#pragma unroll
-      for (int j = 0; j < 16; j++) x[j] = coef[j];
-      compute_groups<K, C, false, BB, VV>(x, tws_fwd, tid, T);
-      store_groups<K, C, BB, VV>(tile, x, tid, T);
-      __syncthreads();
-      rounds_from<K, C, false, false, 1>(tile, tws_fwd, tid, T);
-      uint64_t *out = p.out + (uint64_t)k * p.coset_stride;
-#pragma unroll
-      for (int j = 0; j < 8; j++) {
-        const uint32_t e = 2 * (tid + T * j);
-        uint32_t g;
-        uint64_t off;
-        tile_elem<K, C>(e, g, off, base_off, p.lb);
-        const uint32_t col = c0 + g;
-        if (col >= col_end) continue;
-        uint64_t v0 = tile[pad16(e)], v1 = tile[pad16(e) + 1];
-        if (p.canon_out) {
-          v0 = gl::canon(v0);
-          v1 = gl::canon(v1);
-        }
-        uint64_t *dst = out + (uint64_t)col * p.stride_out + off;
-        if (p.vec_out) {
-          *reinterpret_cast<ulonglong2 *>(dst) = make_ulonglong2(v0, v1);
-        } else {
-          dst[0] = v0;
-          dst[1] = v1;
-        }
-      }
-    }
-    __syncthreads();
-  }
+  top_body<K, C>(p, blockIdx.x, blockIdx.y, smem);
 }
 
 typedef void (*TopKernel)(const LdeTopParams);
+typedef void (*PassKernelT)(const PassParams);
 
 template <int K, int C> static TopKernel tk() { return lde_top_kernel<K, C>; }
 
@@ -218,19 +98,13 @@ bool lde_args_ok(uint32_t log_n, uint32_t num_cols, uint64_t stride_in, uint64_t
   return coset_major || column_major;
 }
 
-// events (optional): ev[0] is recorded before the first kernel and ev[j + 1]
-// after kernel j, for as many events as are given.
-cudaError_t lde_fused(const Plan &pl, const uint64_t *in, uint64_t *out, uint32_t log_n, uint32_t num_cols,
-                      uint64_t stride_in, uint64_t stride_out, uint64_t coset_stride, uint32_t log_blowup,
-                      cudaStream_t stream, cudaEvent_t *ev = nullptr, uint32_t n_ev = 0) {
+bool build_lde_steps(const Plan &pl, const uint64_t *in, uint64_t *out, uint32_t log_n, uint32_t num_cols,
+                     uint64_t stride_in, uint64_t stride_out, uint64_t coset_stride, uint32_t log_blowup,
+                     bool full_tile, int cols_factor_max, std::vector<LdeStep> &steps) {
   const DevTables *tabs = device_tables();
-  if (!tabs) return cudaErrorInitializationError;
-  if (num_cols == 0) return cudaSuccess;
-  uint32_t ev_used = 0;
-  auto mark = [&]() {
-    if (ev_used < n_ev) cudaEventRecord(ev[ev_used++], stream);
-  };
-  mark();
+  if (!tabs) return false;
+  steps.clear();
+  if (num_cols == 0) return true;
   const uint32_t nb = 1u << log_blowup;
   uint64_t *T = out + (uint64_t)(nb - 1) * coset_stride;
   const int np = pl.npasses;
@@ -249,14 +123,22 @@ cudaError_t lde_fused(const Plan &pl, const uint64_t *in, uint64_t *out, uint32_
     q.log_n = log_n;
     q.lb = plan_lb(pl, log_n, i);
     q.inverse = true;
-    cudaError_t e = launch_pass(q, stream);
-    if (e != cudaSuccess) return e;
-    mark();
+    q.full_tile = full_tile;
+    LdeStep st;
+    st.K = q.K;
+    st.C = q.C;
+    st.b2n = true;
+    if (!build_pass(q, cols_factor_max, st.pass, st.grid, st.threads, st.smem)) return false;
+    steps.push_back(st);
   }
   // B: top window
   {
     const int K = pl.pass[0].K, C = pl.pass[0].C;
-    LdeTopParams p{};
+    LdeStep st;
+    st.top = true;
+    st.K = K;
+    st.C = C;
+    LdeTopParams &p = st.topp;
     p.in = np == 1 ? in : T;
     p.out = out;
     p.stride_in = np == 1 ? stride_in : stride_out;
@@ -267,32 +149,25 @@ cudaError_t lde_fused(const Plan &pl, const uint64_t *in, uint64_t *out, uint32_
     p.lb = log_n - K;
     p.log_blowup = log_blowup;
     const uint32_t wc_log = (uint32_t)K + ilog2_ceil((uint32_t)C);
-    p.log_g = choose_log_g(wc_log, num_cols);
+    p.log_g = full_tile ? (wc_log < 12 ? 12 - wc_log : 0) : choose_log_g(wc_log, num_cols);
     const uint32_t G = 1u << p.log_g;
     const uint64_t tiles = (1ull << log_n) >> wc_log;
     const uint64_t chunks = (num_cols + G - 1) / G;
     uint64_t factor = (tiles * chunks) / ((uint64_t)sm_count() * 8);
     if (factor < 1) factor = 1;
-    if (factor > 8) factor = 8;
+    if (factor > (uint64_t)cols_factor_max) factor = cols_factor_max;
     p.cols_per_cta = G * (uint32_t)factor;
     p.canon_out = np == 1;
     p.vec_in = ((uintptr_t)p.in % 16 == 0 && p.stride_in % 2 == 0) ? 1 : 0;
     p.vec_out = ((uintptr_t)out % 16 == 0 && stride_out % 2 == 0 && coset_stride % 2 == 0) ? 1 : 0;
     p.tabs = *tabs;
-    TopKernel kern = pick_top(K, C);
-    if (!kern) return cudaErrorInvalidValue;
     const uint32_t tile = G << wc_log;
-    const size_t smem = ((size_t)tile + tile / 16 + 2 * ((1u << K) - 1)) * sizeof(uint64_t);
-    if (smem > 48 * 1024) {
-      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e != cudaSuccess) return e;
-    }
+    st.threads = tile / 16;
+    st.smem = (size_t)top_smem_words(tile, K) * sizeof(uint64_t);
     const uint64_t gy = (num_cols + p.cols_per_cta - 1) / p.cols_per_cta;
-    if (gy > 65535 || tiles > 0x7fffffffull) return cudaErrorInvalidConfiguration;
-    kern<<<dim3((uint32_t)tiles, (uint32_t)gy), tile / 16, smem, stream>>>(p);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    mark();
+    if (gy > 65535 || tiles > 0x7fffffffull) return false;
+    st.grid = dim3((uint32_t)tiles, (uint32_t)gy);
+    steps.push_back(st);
   }
   // C: forward passes below the top window for all cosets (column groups with prefix brev(k))
   for (int i = 1; i < np; i++) {
@@ -312,9 +187,54 @@ cudaError_t lde_fused(const Plan &pl, const uint64_t *in, uint64_t *out, uint32_
     q.lb = plan_lb(pl, log_n, i);
     q.inverse = false;
     q.canon_out = i == np - 1;
-    cudaError_t e = launch_pass(q, stream);
+    q.full_tile = full_tile;
+    LdeStep st;
+    st.K = q.K;
+    st.C = q.C;
+    if (!build_pass(q, cols_factor_max, st.pass, st.grid, st.threads, st.smem)) return false;
+    steps.push_back(st);
+  }
+  return true;
+}
+
+cudaError_t launch_lde_step(const LdeStep &st, cudaStream_t stream) {
+  if (st.top) {
+    TopKernel kern = pick_top(st.K, st.C);
+    if (!kern) return cudaErrorInvalidValue;
+    if (st.smem > 48 * 1024) {
+      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)st.smem);
+      if (e != cudaSuccess) return e;
+    }
+    kern<<<st.grid, st.threads, st.smem, stream>>>(st.topp);
+  } else {
+    PassKernel kern = pick_pass_kernel(st.K, st.C, st.b2n);
+    if (!kern) return cudaErrorInvalidValue;
+    if (st.smem > 48 * 1024) {
+      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)st.smem);
+      if (e != cudaSuccess) return e;
+    }
+    kern<<<st.grid, st.threads, st.smem, stream>>>(st.pass);
+  }
+  return cudaGetLastError();
+}
+
+// events (optional): ev[0] is recorded before the first kernel and ev[j + 1]
+// after kernel j, for as many events as are given.
+cudaError_t lde_fused(const Plan &pl, const uint64_t *in, uint64_t *out, uint32_t log_n, uint32_t num_cols,
+                      uint64_t stride_in, uint64_t stride_out, uint64_t coset_stride, uint32_t log_blowup,
+                      cudaStream_t stream, cudaEvent_t *ev = nullptr, uint32_t n_ev = 0) {
+  if (!device_tables()) return cudaErrorInitializationError;
+  if (num_cols == 0) return cudaSuccess;
+  std::vector<LdeStep> steps;
+  if (!build_lde_steps(pl, in, out, log_n, num_cols, stride_in, stride_out, coset_stride, log_blowup, false, 8,
+                       steps))
+    return cudaErrorInvalidConfiguration;
+  uint32_t ev_used = 0;
+  if (ev_used < n_ev) cudaEventRecord(ev[ev_used++], stream);
+  for (const LdeStep &st : steps) {
+    cudaError_t e = launch_lde_step(st, stream);
     if (e != cudaSuccess) return e;
-    mark();
+    if (ev_used < n_ev) cudaEventRecord(ev[ev_used++], stream);
   }
   return cudaSuccess;
 }

@@ -1,0 +1,170 @@
+// lde.cuh -- the fused LDE's top-window kernel body and its step description.
+//
+// See lde.cu for the algorithm.  The body is shared by the standalone
+// lde_top_kernel launch and by the persistent batch kernel (lde_batch.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "ntt_host.cuh"
+#include "ntt_pass.cuh"
+
+namespace bc {
+
+struct LdeTopParams {
+  const uint64_t *in; // T (or the evaluations when the plan has one pass)
+  uint64_t *out;      // coset block 0
+  uint64_t stride_in;
+  uint64_t stride_out;
+  uint64_t coset_stride;
+  uint32_t num_cols;
+  uint32_t log_n;
+  uint32_t lb; // = log_n - K
+  uint32_t log_blowup;
+  uint32_t log_g;
+  uint32_t cols_per_cta;
+  uint32_t canon_out; // single-pass plan: this kernel writes final values
+  uint32_t vec_in, vec_out;
+  DevTables tabs;
+};
+
+// One CTA's work of the top-window kernel: tile position bx (run of low
+// positions), column chunk by.  blockDim.x == 2^log_g * 2^K * C / 16.
+template <int K, int C>
+__device__ __forceinline__ void top_body(const LdeTopParams &p, uint32_t bx, uint32_t by, uint64_t *smem) {
+  constexpr int W = 1 << K;
+  using LastInv = RoundShape<K, true, true, (K + 3) / 4 - 1>; // last inverse round ...
+  using FirstFwd = RoundShape<K, false, false, 0>;            // ... holds the first forward round's groups
+  static_assert(LastInv::B == FirstFwd::B && LastInv::V == FirstFwd::V, "round hand-over mismatch");
+  constexpr int BB = FirstFwd::B, VV = FirstFwd::V, NV = 1 << VV, NG = 16 / NV;
+  const uint32_t G = 1u << p.log_g;
+  const uint32_t TILE = G * W * C;
+  const uint32_t T = TILE / 16;
+  uint64_t *tile = smem;
+  uint64_t *tws_inv = smem + TILE + TILE / 16;
+  uint64_t *tws_fwd = tws_inv + TwSlots<K>::words;
+  const uint32_t tid = threadIdx.x;
+
+  // top window: H = 0, the tile position is the run of low positions
+  const uint64_t base_off = (uint64_t)bx << LogC<C>::v;
+  const uint32_t col_begin = by * p.cols_per_cta;
+  const uint32_t col_end = min(p.num_cols, col_begin + p.cols_per_cta);
+  fill_twiddles<K>(tws_inv, p.tabs, 1, 0, tid, T);
+
+  // scale n^-1 g^i of this thread's groups: i = base + lc + (w_j << lb), w_j = w | (j << BB)
+  const uint64_t g_step = g_power(p.tabs, 0, 1u << (p.lb + BB));
+  const uint64_t inv_n = p.tabs.inv_pow2[p.log_n];
+  const uint32_t nb = 1u << p.log_blowup;
+
+  for (uint32_t c0 = col_begin; c0 < col_end; c0 += G) {
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+      const uint32_t e = 2 * (tid + T * j);
+      uint32_t g;
+      uint64_t off;
+      tile_elem<K, C>(e, g, off, base_off, p.lb);
+      const uint32_t col = c0 + g;
+      uint64_t v0 = 0, v1 = 0;
+      if (col < col_end) {
+        const uint64_t *src = p.in + (uint64_t)col * p.stride_in + off;
+        if (p.vec_in) {
+          const ulonglong2 v = __ldcg(reinterpret_cast<const ulonglong2 *>(src));
+          v0 = v.x;
+          v1 = v.y;
+        } else {
+          v0 = __ldcg(src);
+          v1 = __ldcg(src + 1);
+        }
+      }
+      tile[pad16(e)] = v0;
+      tile[pad16(e) + 1] = v1;
+    }
+    __syncthreads();
+
+    // inverse stages of the window (bottom-up), all but the last round through shared memory
+    rounds_from<K, C, true, true, 0, (K + 3) / 4 - 1>(tile, tws_inv, tid, T);
+    uint64_t coef[16];
+    load_groups<K, C, BB, VV>(tile, coef, tid, T);
+    compute_groups<K, C, true, BB, VV>(coef, tws_inv, tid, T);
+#pragma unroll
+    for (int q = 0; q < NG; q++) {
+      uint32_t w;
+      const uint32_t gi = tid + T * q;
+      group_base<K, C, BB, VV>(gi, w);
+      const uint32_t i0 = (uint32_t)base_off + gi % C + (w << p.lb);
+      uint64_t s = gl::mul(inv_n, g_power(p.tabs, 0, i0));
+#pragma unroll
+      for (int j = 0; j < NV; j++) {
+        coef[q * NV + j] = gl::mul(coef[q * NV + j], s);
+        if (j + 1 < NV) s = gl::mul(s, g_step);
+      }
+    }
+
+    for (uint32_t k = 0; k < nb; k++) {
+      __syncthreads(); // previous coset's stores have read the tile and twiddles
+      fill_twiddles<K>(tws_fwd, p.tabs, 0, brev_bits(k, p.log_blowup), tid, T);
+      __syncthreads();
+      uint64_t x[16];
+#pragma unroll
+      for (int j = 0; j < 16; j++) x[j] = coef[j];
+      compute_groups<K, C, false, BB, VV>(x, tws_fwd, tid, T);
+      store_groups<K, C, BB, VV>(tile, x, tid, T);
+      __syncthreads();
+      rounds_from<K, C, false, false, 1>(tile, tws_fwd, tid, T);
+      uint64_t *out = p.out + (uint64_t)k * p.coset_stride;
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        const uint32_t e = 2 * (tid + T * j);
+        uint32_t g;
+        uint64_t off;
+        tile_elem<K, C>(e, g, off, base_off, p.lb);
+        const uint32_t col = c0 + g;
+        if (col >= col_end) continue;
+        uint64_t v0 = tile[pad16(e)], v1 = tile[pad16(e) + 1];
+        if (p.canon_out) {
+          v0 = gl::canon(v0);
+          v1 = gl::canon(v1);
+        }
+        uint64_t *dst = out + (uint64_t)col * p.stride_out + off;
+        if (p.vec_out) {
+          *reinterpret_cast<ulonglong2 *>(dst) = make_ulonglong2(v0, v1);
+        } else {
+          dst[0] = v0;
+          dst[1] = v1;
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+__host__ __device__ constexpr uint32_t top_smem_words(uint32_t tile, int K) {
+  return tile + tile / 16 + 2 * ((1u << K) + (1u << K) / 16);
+}
+
+// One kernel of a fused LDE: either a pass (ntt_pass_kernel) or the top-window
+// kernel, with its parameters and launch shape.
+struct LdeStep {
+  bool top = false;
+  int K = 0, C = 1;
+  bool b2n = false;
+  PassParams pass{};
+  LdeTopParams topp{};
+  dim3 grid;
+  uint32_t threads = 0;
+  size_t smem = 0;
+};
+
+// Steps of one fused LDE (inverse passes below the top window, the top-window
+// kernel, forward passes below it).  full_tile: 4096-element tiles (256
+// threads) for every step; cols_factor_max: column groups per CTA.
+bool build_lde_steps(const Plan &pl, const uint64_t *in, uint64_t *out, uint32_t log_n, uint32_t num_cols,
+                     uint64_t stride_in, uint64_t stride_out, uint64_t coset_stride, uint32_t log_blowup,
+                     bool full_tile, int cols_factor_max, std::vector<LdeStep> &steps);
+
+bool lde_args_ok(uint32_t log_n, uint32_t num_cols, uint64_t stride_in, uint64_t stride_out, uint64_t coset_stride,
+                 uint32_t log_blowup);
+
+} // namespace bc

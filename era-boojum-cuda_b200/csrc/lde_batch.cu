@@ -1,0 +1,321 @@
+// lde_batch.cu -- uneven batches of coset LDE jobs in ONE persistent launch.
+//
+// The reference has no batch entry point: its callers issue one inverse and
+// one forward batch_ntt per coset per job (src/ntt.rs:179-191), and for
+// log_n < 16 every stage is its own launch (src/ntt.rs:201-241), so a batch of
+// small, uneven jobs is dominated by launch latency and tail effects.
+//
+// Here a batch plan turns every job's fused LDE (lde.cu: inverse passes,
+// top-window kernel, forward passes) into "records" -- one per kernel of the
+// job, each holding exactly the parameters the standalone launch would get --
+// and every record into work items, one per CTA of that launch.  Records are
+// ordered by depth (first kernels of all jobs, then second kernels, ...) and
+// items by record, so every item depends only on items earlier in the list.
+// One persistent kernel (grid = resident CTAs) pulls items with an atomic
+// counter; before an item of a job's k-th kernel it waits until all items of
+// the job's (k-1)-th kernel are done.  Because items are taken in list order
+// and every earlier item is held by a running CTA, the waits always end.  Each
+// wait is still bounded in time: on expiry the kernel sets a status bit,
+// skips the item and carries on, so a fault can never hang the GPU.
+//
+// The launch (counter reset + kernel) is captured once per plan in a CUDA
+// graph and replayed by bc_lde_batch_run.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "../../include/bc_ntt.h"
+#include "lde.cuh"
+
+namespace bc {
+
+// Dispatch id of a kernel body: (top << 7) | (b2n << 6) | (K << 2) | log2(C).
+__host__ __device__ constexpr uint32_t shape_id(bool top, bool b2n, int K, int C) {
+  return ((top ? 1u : 0u) << 7) | ((b2n ? 1u : 0u) << 6) | ((uint32_t)K << 2) |
+         (C == 1 ? 0u : C == 2 ? 1u : C == 4 ? 2u : 3u);
+}
+
+struct BatchRecord {
+  uint32_t shape;
+  int32_t pred;     // record that must be complete before any item of this one, or -1
+  uint32_t n_items; // CTAs of this kernel
+  uint32_t pad;
+  union {
+    PassParams pass;
+    LdeTopParams top;
+  } u;
+};
+
+// item = record (16 bits) | column chunk by (20 bits) | tile position bx (28 bits)
+__host__ __device__ constexpr uint64_t make_item(uint32_t rec, uint32_t by, uint32_t bx) {
+  return ((uint64_t)rec << 48) | ((uint64_t)by << 28) | (uint64_t)bx;
+}
+
+constexpr uint32_t BATCH_THREADS = 256;
+constexpr uint32_t BATCH_SMEM_BYTES = top_smem_words(4096, 12) * 8; // largest body: top window of 12 bits
+
+// The bodies the persistent kernel can run: every window shape of the default
+// plans (and of the tuner's candidates).
+#define BC_BATCH_SHAPES(X)                                                                                           \
+  X(true, false, 1, 1) X(true, false, 2, 1) X(true, false, 3, 1) X(true, false, 4, 1) X(true, false, 5, 1)        \
+  X(true, false, 6, 1) X(true, false, 7, 1) X(true, false, 8, 1) X(true, false, 9, 1) X(true, false, 10, 1)       \
+  X(true, false, 11, 1) X(true, false, 12, 1) X(true, false, 4, 8) X(true, false, 5, 8) X(true, false, 8, 8)      \
+  X(true, false, 9, 8) X(true, false, 10, 4) X(true, false, 11, 2)                                                 \
+  X(false, true, 8, 1) X(false, true, 9, 1) X(false, true, 10, 1) X(false, true, 11, 1) X(false, true, 12, 1)     \
+  X(false, false, 8, 1) X(false, false, 9, 1) X(false, false, 10, 1) X(false, false, 11, 1)                         \
+  X(false, false, 12, 1) X(false, true, 8, 8) X(false, true, 9, 8) X(false, true, 10, 4) X(false, false, 8, 8)    \
+  X(false, false, 9, 8) X(false, false, 10, 4)
+
+bool batch_shape_supported(uint32_t id) {
+#define BC_CASE(TOP, B2N, K, C)                                                                                      \
+  if (id == shape_id(TOP, B2N, K, C)) return true;
+  BC_BATCH_SHAPES(BC_CASE)
+#undef BC_CASE
+  return false;
+}
+
+template <bool TOP, bool B2N, int K, int C>
+__device__ __noinline__ void run_shape(const BatchRecord &rec, uint32_t bx, uint32_t by, uint64_t *smem) {
+  if constexpr (TOP)
+    top_body<K, C>(rec.u.top, bx, by, smem);
+  else
+    pass_body<K, C, B2N>(rec.u.pass, bx, by, smem);
+}
+
+__device__ __forceinline__ void run_body(const BatchRecord &rec, uint32_t bx, uint32_t by, uint64_t *smem) {
+  switch (rec.shape) {
+#define BC_CASE(TOP, B2N, K, C)                                                                                      \
+  case shape_id(TOP, B2N, K, C):                                                                                     \
+    run_shape<TOP, B2N, K, C>(rec, bx, by, smem);                                                                    \
+    break;
+    BC_BATCH_SHAPES(BC_CASE)
+#undef BC_CASE
+  default:
+    break;
+  }
+}
+
+__device__ __forceinline__ uint32_t ld_acquire(const uint32_t *p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// status bit 0: a dependency wait expired (the batch's results are invalid).
+__global__ void __launch_bounds__(BATCH_THREADS, 2)
+    lde_batch_kernel(const BatchRecord *__restrict__ recs, const uint64_t *__restrict__ items, uint32_t n_items,
+                     uint32_t *done, uint32_t *next, uint32_t *status, long long timeout_cycles) {
+  extern __shared__ uint64_t smem[];
+  __shared__ uint32_t s_idx, s_ok;
+  __shared__ BatchRecord s_rec; // the item's kernel parameters, read by the body from shared memory
+  for (;;) {
+    if (threadIdx.x == 0) s_idx = atomicAdd(next, 1u);
+    __syncthreads();
+    const uint32_t idx = s_idx;
+    if (idx >= n_items) return;
+    const uint64_t it = items[idx];
+    const uint32_t r = (uint32_t)(it >> 48), by = (uint32_t)(it >> 28) & 0xFFFFFu, bx = (uint32_t)it & 0xFFFFFFFu;
+    const BatchRecord &rec = recs[r];
+    static_assert(sizeof(BatchRecord) % 4 == 0, "record copy by words");
+    for (uint32_t w = threadIdx.x; w < sizeof(BatchRecord) / 4; w += blockDim.x)
+      reinterpret_cast<uint32_t *>(&s_rec)[w] = reinterpret_cast<const uint32_t *>(&rec)[w];
+    if (threadIdx.x == 0) {
+      uint32_t ok = 1;
+      if (rec.pred >= 0) {
+        const uint32_t need = recs[rec.pred].n_items;
+        const long long t0 = clock64();
+        while (ld_acquire(done + rec.pred) < need) {
+          if (clock64() - t0 > timeout_cycles) {
+            ok = 0;
+            atomicOr(status, 1u);
+            break;
+          }
+          __nanosleep(128);
+        }
+      }
+      s_ok = ok;
+    }
+    __syncthreads();
+    if (s_ok) run_body(s_rec, bx, by, smem);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      atomicAdd(done + r, 1u);
+    }
+  }
+}
+
+} // namespace bc
+
+using namespace bc;
+
+struct bc_lde_batch_plan {
+  int device = -1;
+  uint32_t n_records = 0, n_items = 0, grid = 0;
+  BatchRecord *d_records = nullptr;
+  uint64_t *d_items = nullptr;
+  uint32_t *d_counters = nullptr; // done[n_records], next, status
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  long long timeout_cycles = 0;
+};
+
+namespace {
+
+cudaError_t free_plan(bc_lde_batch_plan *p) {
+  if (!p) return cudaSuccess;
+  cudaError_t e = cudaSuccess, e2;
+  if (p->exec && (e2 = cudaGraphExecDestroy(p->exec)) != cudaSuccess) e = e2;
+  if (p->graph && (e2 = cudaGraphDestroy(p->graph)) != cudaSuccess) e = e2;
+  if (p->d_records && (e2 = cudaFree(p->d_records)) != cudaSuccess) e = e2;
+  if (p->d_items && (e2 = cudaFree(p->d_items)) != cudaSuccess) e = e2;
+  if (p->d_counters && (e2 = cudaFree(p->d_counters)) != cudaSuccess) e = e2;
+  delete p;
+  return e;
+}
+
+uint64_t job_work(const bc_lde_job &j) { return ((uint64_t)j.num_cols << j.log_n) << j.log_blowup; }
+
+// Records and items of a batch, in dependency order (host side).
+cudaError_t schedule(const bc_lde_job *jobs, uint32_t n_jobs, std::vector<BatchRecord> &recs,
+                     std::vector<uint64_t> &items) {
+  std::vector<std::vector<LdeStep>> steps(n_jobs);
+  size_t max_depth = 0;
+  for (uint32_t j = 0; j < n_jobs; j++) {
+    const bc_lde_job &jb = jobs[j];
+    if (!lde_args_ok(jb.log_n, jb.num_cols, jb.stride_in, jb.stride_out, jb.coset_stride, jb.log_blowup))
+      return cudaErrorInvalidValue;
+    if (jb.num_cols && (!jb.evals_bitrev || !jb.out)) return cudaErrorInvalidValue;
+    if (!build_lde_steps(default_plan(jb.log_n), jb.evals_bitrev, jb.out, jb.log_n, jb.num_cols, jb.stride_in,
+                         jb.stride_out, jb.coset_stride, jb.log_blowup, true, 4, steps[j]))
+      return cudaErrorInvalidConfiguration;
+    for (const LdeStep &st : steps[j]) {
+      if (!batch_shape_supported(shape_id(st.top, st.b2n, st.K, st.C)) || st.threads != BATCH_THREADS ||
+          st.smem > BATCH_SMEM_BYTES || st.grid.x >= (1u << 28) || st.grid.y >= (1u << 20))
+        return cudaErrorInvalidConfiguration;
+    }
+    max_depth = std::max(max_depth, steps[j].size());
+  }
+  // big jobs first within every depth
+  std::vector<uint32_t> order(n_jobs);
+  for (uint32_t j = 0; j < n_jobs; j++) order[j] = j;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](uint32_t a, uint32_t b) { return job_work(jobs[a]) > job_work(jobs[b]); });
+  std::vector<int32_t> last(n_jobs, -1);
+  recs.clear();
+  items.clear();
+  for (size_t d = 0; d < max_depth; d++) {
+    for (uint32_t j : order) {
+      if (d >= steps[j].size()) continue;
+      const LdeStep &st = steps[j][d];
+      BatchRecord r;
+      std::memset(&r, 0, sizeof(r));
+      r.shape = shape_id(st.top, st.b2n, st.K, st.C);
+      r.pred = last[j];
+      r.n_items = st.grid.x * st.grid.y;
+      if (st.top)
+        r.u.top = st.topp;
+      else
+        r.u.pass = st.pass;
+      const uint32_t rid = (uint32_t)recs.size();
+      if (rid >= (1u << 16)) return cudaErrorInvalidConfiguration;
+      recs.push_back(r);
+      last[j] = (int32_t)rid;
+      for (uint32_t by = 0; by < st.grid.y; by++)
+        for (uint32_t bx = 0; bx < st.grid.x; bx++) items.push_back(make_item(rid, by, bx));
+    }
+  }
+  if (items.size() >= (1ull << 32)) return cudaErrorInvalidConfiguration;
+  return cudaSuccess;
+}
+
+} // namespace
+
+extern "C" cudaError_t bc_lde_batch_plan_create(const bc_lde_job *jobs, uint32_t n_jobs, bc_lde_batch_plan **plan) {
+  if (!plan || (n_jobs && !jobs)) return cudaErrorInvalidValue;
+  *plan = nullptr;
+  if (!device_tables()) return cudaErrorInitializationError;
+  std::vector<BatchRecord> recs;
+  std::vector<uint64_t> items;
+  cudaError_t e = schedule(jobs, n_jobs, recs, items);
+  if (e != cudaSuccess) return e;
+  bc_lde_batch_plan *p = new (std::nothrow) bc_lde_batch_plan();
+  if (!p) return cudaErrorMemoryAllocation;
+  p->device = current_device();
+  p->n_records = (uint32_t)recs.size();
+  p->n_items = (uint32_t)items.size();
+  int dev_clock_khz = 0;
+  cudaDeviceGetAttribute(&dev_clock_khz, cudaDevAttrClockRate, p->device);
+  p->timeout_cycles = (long long)std::max(dev_clock_khz, 1000000) * 1000ll * 4; // ~4 s of SM clock per wait
+#define CK(x)                                                                                                          \
+  if ((e = (x)) != cudaSuccess) {                                                                                      \
+    free_plan(p);                                                                                                      \
+    return e;                                                                                                          \
+  }
+  CK(cudaFuncSetAttribute(lde_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)BATCH_SMEM_BYTES));
+  int per_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lde_batch_kernel, BATCH_THREADS, BATCH_SMEM_BYTES));
+  if (per_sm < 1) {
+    free_plan(p);
+    return cudaErrorInvalidConfiguration;
+  }
+  p->grid = (uint32_t)(per_sm * sm_count());
+  if (p->n_records) {
+    CK(cudaMalloc(&p->d_records, recs.size() * sizeof(BatchRecord)));
+    CK(cudaMemcpy(p->d_records, recs.data(), recs.size() * sizeof(BatchRecord), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&p->d_items, items.size() * sizeof(uint64_t)));
+    CK(cudaMemcpy(p->d_items, items.data(), items.size() * sizeof(uint64_t), cudaMemcpyHostToDevice));
+  }
+  CK(cudaMalloc(&p->d_counters, (p->n_records + 2) * sizeof(uint32_t)));
+  CK(cudaMemset(p->d_counters, 0, (p->n_records + 2) * sizeof(uint32_t)));
+  // capture: reset the counters, run the persistent kernel
+  cudaStream_t cs;
+  CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+  e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    cudaMemsetAsync(p->d_counters, 0, (p->n_records + 2) * sizeof(uint32_t), cs);
+    if (p->n_items)
+      lde_batch_kernel<<<p->grid, BATCH_THREADS, BATCH_SMEM_BYTES, cs>>>(
+          p->d_records, p->d_items, p->n_items, p->d_counters, p->d_counters + p->n_records,
+          p->d_counters + p->n_records + 1, p->timeout_cycles);
+    e = cudaStreamEndCapture(cs, &p->graph);
+  }
+  cudaStreamDestroy(cs);
+  if (e != cudaSuccess) {
+    free_plan(p);
+    return e;
+  }
+  CK(cudaGraphInstantiate(&p->exec, p->graph, 0));
+#undef CK
+  *plan = p;
+  return cudaSuccess;
+}
+
+extern "C" cudaError_t bc_lde_batch_run(bc_lde_batch_plan *plan, cudaStream_t stream) {
+  if (!plan) return cudaErrorInvalidValue;
+  if (current_device() != plan->device) return cudaErrorInvalidDevice;
+  return cudaGraphLaunch(plan->exec, stream);
+}
+
+extern "C" cudaError_t bc_lde_batch_status(bc_lde_batch_plan *plan, cudaStream_t stream, uint32_t *status) {
+  if (!plan || !status) return cudaErrorInvalidValue;
+  cudaError_t e = cudaMemcpyAsync(status, plan->d_counters + plan->n_records + 1, sizeof(uint32_t),
+                                  cudaMemcpyDeviceToHost, stream);
+  if (e != cudaSuccess) return e;
+  return cudaStreamSynchronize(stream);
+}
+
+extern "C" cudaError_t bc_lde_batch_plan_info(const bc_lde_batch_plan *plan, uint32_t *n_records, uint32_t *n_items,
+                                              uint32_t *grid) {
+  if (!plan) return cudaErrorInvalidValue;
+  if (n_records) *n_records = plan->n_records;
+  if (n_items) *n_items = plan->n_items;
+  if (grid) *grid = plan->grid;
+  return cudaSuccess;
+}
+
+extern "C" cudaError_t bc_lde_batch_plan_destroy(bc_lde_batch_plan *plan) { return free_plan(plan); }

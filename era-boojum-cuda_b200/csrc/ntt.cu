@@ -159,31 +159,30 @@ cudaError_t context_destroy_current() {
 }
 
 // ---------------------------------------------------------------- plans
+// Default pass plans.  The pass that owns bit 0 takes up to 12 bits (contiguous
+// 32 KB tiles); the others use windows whose shared-memory rounds are free of
+// bank conflicts: 4, 5, 8 or 9 bits with runs of 8 (64-byte rows), 10 bits with
+// runs of 4, 11 bits with runs of 2.
 Plan default_plan(uint32_t log_n) {
   Plan pl{};
-  auto c_for = [](int K) -> uint8_t { return K <= 9 ? 8 : K == 10 ? 4 : 2; };
+  auto run_for = [](int K) -> uint8_t { return K <= 9 ? 8 : K == 10 ? 4 : 2; };
+  // top window bits for 13..23 (index log_n - 13), then 12 bits at the bottom
+  static const uint8_t top2[11] = {5, 5, 5, 8, 8, 9, 9, 9, 9, 10, 11};
+  static const uint8_t low2[11] = {8, 9, 10, 8, 9, 9, 10, 11, 12, 12, 12};
   if (log_n <= 12) {
     pl.npasses = 1;
     pl.pass[0] = {(uint8_t)log_n, 1};
-  } else if (log_n <= 21) {
-    int k_last = (int)(log_n + 1) / 2;
-    if (k_last < (int)log_n - 9) k_last = (int)log_n - 9;
-    if (k_last > 12) k_last = 12;
-    const int k1 = (int)log_n - k_last;
-    pl.npasses = 2;
-    pl.pass[0] = {(uint8_t)k1, c_for(k1)};
-    pl.pass[1] = {(uint8_t)k_last, 1};
   } else if (log_n <= 23) {
-    const int k1 = (int)log_n - 12;
     pl.npasses = 2;
-    pl.pass[0] = {(uint8_t)k1, c_for(k1)};
-    pl.pass[1] = {12, 1};
+    const int k1 = top2[log_n - 13], k2 = low2[log_n - 13];
+    pl.pass[0] = {(uint8_t)k1, run_for(k1)};
+    pl.pass[1] = {(uint8_t)k2, 1};
   } else {
-    const int rest = (int)log_n - 12;
-    const int k0 = rest / 2, k1 = rest - k0;
+    // 24..27: two upper windows from {4, 5, 8, 9, 10} over the bits above 12
+    static const uint8_t a3[4] = {4, 5, 5, 5}, b3[4] = {8, 8, 9, 10};
     pl.npasses = 3;
-    pl.pass[0] = {(uint8_t)k0, c_for(k0)};
-    pl.pass[1] = {(uint8_t)k1, c_for(k1)};
+    pl.pass[0] = {a3[log_n - 24], run_for(a3[log_n - 24])};
+    pl.pass[1] = {b3[log_n - 24], run_for(b3[log_n - 24])};
     pl.pass[2] = {12, 1};
   }
   return pl;
@@ -219,7 +218,6 @@ bool plan_valid(const Plan &pl, uint32_t log_n) {
 }
 
 // ---------------------------------------------------------------- kernels
-typedef void (*PassKernel)(const PassParams);
 
 template <int K, int C, bool B2N> static PassKernel kptr() { return ntt_pass_kernel<K, C, B2N>; }
 
@@ -256,7 +254,7 @@ template <bool B2N> static PassKernel pick_c8(int K) {
   }
 }
 
-static PassKernel pick_kernel(int K, int C, bool b2n) {
+PassKernel pick_pass_kernel(int K, int C, bool b2n) {
   if (C == 1) return b2n ? pick_c1<true>(K) : pick_c1<false>(K);
   if (C == 8) return b2n ? pick_c8<true>(K) : pick_c8<false>(K);
   if (C == 4 && K == 10) return b2n ? kptr<10, 4, true>() : kptr<10, 4, false>();
@@ -294,12 +292,12 @@ uint32_t choose_log_g(uint32_t wc_log, uint32_t cols) {
   return log_g;
 }
 
-cudaError_t launch_pass(const PassLaunch &pl, cudaStream_t stream) {
+bool build_pass(const PassLaunch &pl, int cols_factor_max, PassParams &p, dim3 &grid, uint32_t &threads,
+                size_t &smem_bytes) {
   const DevTables *tabs = device_tables();
-  if (!tabs) return cudaErrorInitializationError;
-  if (pl.cols == 0) return cudaSuccess;
+  if (!tabs) return false;
   const int K = pl.K, C = pl.C;
-  PassParams p{};
+  p = PassParams{};
   p.in = pl.in;
   p.out = pl.out;
   p.stride_in = pl.stride_in;
@@ -311,14 +309,14 @@ cudaError_t launch_pass(const PassLaunch &pl, cudaStream_t stream) {
   p.log_n = pl.log_n;
   p.lb = pl.lb;
   const uint32_t wc_log = (uint32_t)K + log2_ceil((uint32_t)C);
-  p.log_g = choose_log_g(wc_log, pl.cols);
+  p.log_g = pl.full_tile ? (wc_log < 12 ? 12 - wc_log : 0) : choose_log_g(wc_log, pl.cols);
   const uint32_t G = 1u << p.log_g;
   const uint64_t tiles_per_col = (1ull << pl.log_n) >> wc_log;
   const uint64_t groups = 1ull << pl.log_groups;
   const uint64_t chunks = (pl.cols + G - 1) / G;
   uint64_t factor = (tiles_per_col * chunks * groups) / ((uint64_t)sm_count() * 8);
   if (factor < 1) factor = 1;
-  if (factor > 8) factor = 8;
+  if (factor > (uint64_t)cols_factor_max) factor = cols_factor_max;
   p.cols_per_cta = G * (uint32_t)factor;
   p.chunks_per_group = (pl.cols + p.cols_per_cta - 1) / p.cols_per_cta;
   p.inverse = pl.inverse;
@@ -330,18 +328,29 @@ cudaError_t launch_pass(const PassLaunch &pl, cudaStream_t stream) {
   p.vec_in = ((uintptr_t)p.in % 16 == 0 && p.stride_in % 2 == 0 && p.group_stride_in % 2 == 0) ? 1 : 0;
   p.vec_out = ((uintptr_t)p.out % 16 == 0 && p.stride_out % 2 == 0 && p.group_stride_out % 2 == 0) ? 1 : 0;
   p.tabs = *tabs;
-  PassKernel kern = pick_kernel(K, C, pl.b2n);
-  if (!kern) return cudaErrorInvalidValue;
   const uint32_t tile = G << wc_log;
-  const uint32_t threads = tile / 16;
-  const size_t smem = ((size_t)tile + tile / 16 + (1u << K) - 1) * sizeof(uint64_t);
+  threads = tile / 16;
+  smem_bytes = (size_t)pass_smem_words(tile, K) * sizeof(uint64_t);
+  const uint64_t gy = groups * p.chunks_per_group;
+  if (tiles_per_col > 0x7fffffffull || gy > 65535) return false;
+  grid = dim3((uint32_t)tiles_per_col, (uint32_t)gy);
+  return true;
+}
+
+cudaError_t launch_pass(const PassLaunch &pl, cudaStream_t stream) {
+  if (!device_tables()) return cudaErrorInitializationError;
+  if (pl.cols == 0) return cudaSuccess;
+  PassParams p;
+  dim3 grid;
+  uint32_t threads;
+  size_t smem;
+  if (!build_pass(pl, 8, p, grid, threads, smem)) return cudaErrorInvalidConfiguration;
+  PassKernel kern = pick_pass_kernel(pl.K, pl.C, pl.b2n);
+  if (!kern) return cudaErrorInvalidValue;
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
   }
-  const uint64_t gy = groups * p.chunks_per_group;
-  if (tiles_per_col > 0x7fffffffull || gy > 65535) return cudaErrorInvalidConfiguration;
-  dim3 grid((uint32_t)tiles_per_col, (uint32_t)gy);
   kern<<<grid, threads, smem, stream>>>(p);
   return cudaGetLastError();
 }

@@ -45,8 +45,19 @@ struct PassLaunch {
   uint32_t log_n = 0, lb = 0;
   bool inverse = false, load_scale = false, store_scale = false, canon_out = false;
   uint32_t has_coset = 0, coset_kshift = 0;
+  bool full_tile = false; // always 4096-element tiles (256 threads), as the batch kernel runs them
 };
 cudaError_t launch_pass(const PassLaunch &pl, cudaStream_t stream);
+
+struct PassParams;
+// Kernel parameters, grid, block size and shared memory of one pass (no launch).
+// cols_factor_max bounds how many column groups one CTA walks.
+bool build_pass(const PassLaunch &pl, int cols_factor_max, PassParams &p, dim3 &grid, uint32_t &threads,
+                size_t &smem_bytes);
+
+typedef void (*PassKernel)(const PassParams);
+// The standalone pass kernel for a window shape (nullptr when not instantiated).
+PassKernel pick_pass_kernel(int K, int C, bool b2n);
 
 // Window start (lowest bit) of pass i of a plan, passes listed top-down.
 uint32_t plan_lb(const Plan &pl, uint32_t log_n, int i);

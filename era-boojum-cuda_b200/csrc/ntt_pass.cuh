@@ -12,6 +12,9 @@
 // r = idx >> (a + 1) uses twiddle T[r] (see tables.cuh); T[r] does not depend
 // on the stage, exactly as in the reference (native/ntt.cu:23-35).
 //
+// Tile loads bypass L1 (ld.global.cg): a tile is read once, and in the
+// persistent batch kernel another SM may have written it during this launch.
+//
 // Tile.  A CTA owns one tile position: the bits above the window (H) and a
 // run of C consecutive values of the bits below it (l0 .. l0 + C - 1), and
 // walks over columns G at a time.  A tile is G x 2^K x C elements, loaded
@@ -36,6 +39,12 @@
 #pragma once
 #include "gl.cuh"
 #include "tables.cuh"
+
+// Resident CTAs per SM the pass kernels are compiled for (256 threads each);
+// 2 leaves each thread 128 registers, enough for 16 values without spills.
+#ifndef BC_PASS_MIN_BLOCKS
+#define BC_PASS_MIN_BLOCKS 2
+#endif
 
 namespace bc {
 
@@ -114,14 +123,30 @@ __device__ __forceinline__ void dif(uint64_t &a, uint64_t &b, uint64_t t) {
 // A round holds the V window bits [B, B + V) of 16 / 2^V groups per thread in
 // registers: x[q * 2^V + j] is element j of the thread's q-th group.
 
+// Which index runs fastest across consecutive threads of a round.  Runs of C
+// low positions first keeps a half-warp on 16 distinct banks for every full
+// round; a short round on the window's bottom bits with C > 1 instead needs
+// the other window bits first (group stride 2^V * C <= 16 words).
+template <int C, int B, int V> struct GroupOrder {
+  static constexpr bool window_first = (V < 4) && (B == 0) && (C > 1) && ((1 << V) * C <= 16);
+};
+
 // Tile index of element 0 of group gi, and its window value w (bits [B, B+V) zero).
 template <int K, int C, int B, int V>
 __device__ __forceinline__ uint32_t group_base(uint32_t gi, uint32_t &w) {
   constexpr int W = 1 << K;
-  const uint32_t lc = gi % C;
-  const uint32_t rest = gi / C;
-  const uint32_t g = rest >> (K - V);
-  const uint32_t wo = rest & ((1u << (K - V)) - 1);
+  uint32_t lc, g, wo;
+  if constexpr (GroupOrder<C, B, V>::window_first) {
+    wo = gi & ((1u << (K - V)) - 1);
+    const uint32_t rest = gi >> (K - V);
+    lc = rest % C;
+    g = rest / C;
+  } else {
+    lc = gi % C;
+    const uint32_t rest = gi / C;
+    g = rest >> (K - V);
+    wo = rest & ((1u << (K - V)) - 1);
+  }
   w = (wo & ((1u << B) - 1)) | ((wo >> B) << (B + V));
   return (g * W + w) * C + lc;
 }
@@ -150,9 +175,17 @@ __device__ __forceinline__ void store_groups(uint64_t *tile, const uint64_t (&x)
   }
 }
 
+// Shared-memory twiddle slot of entry i: level L (2^L entries) starts at 2^L
+// (entry 0 unused) and one pad word follows every 16, which keeps every
+// round's twiddle reads on distinct banks.
+__device__ __forceinline__ uint32_t tw_slot(uint32_t i) { return i + (i >> 4); }
+template <int K> struct TwSlots {
+  static constexpr uint32_t words = (1u << K) + (1u << K) / 16;
+};
+
 // Stages of one round.  DIF: bottom bit first, (a+b, (a-b)t); DIT: top bit
 // first, (a+bt, a-bt).  Twiddle of window bit qb for upper window part u:
-// tws[2^(K-1-qb) - 1 + u].
+// entry 2^(K-1-qb) + u of the tile's twiddle table.
 template <int K, int C, bool DIF, int B, int V>
 __device__ __forceinline__ void compute_groups(uint64_t (&x)[16], const uint64_t *tws, uint32_t tid,
                                                uint32_t nthreads) {
@@ -169,7 +202,7 @@ __device__ __forceinline__ void compute_groups(uint64_t (&x)[16], const uint64_t
       for (int j0 = 0; j0 < NV; j0++) {
         if (j0 & (1 << qq)) continue;
         const uint32_t u = (w | ((uint32_t)j0 << B)) >> (qb + 1);
-        const uint64_t t = tws[(1u << (K - 1 - qb)) - 1 + u];
+        const uint64_t t = tws[tw_slot((1u << (K - 1 - qb)) + u)];
         if (DIF)
           dif(x[q * NV + j0], x[q * NV + (j0 | (1 << qq))], t);
         else
@@ -207,15 +240,15 @@ __device__ __forceinline__ void rounds_from(uint64_t *tile, const uint64_t *tws,
   }
 }
 
-// Shared-memory twiddles of one tile position: entry 2^(K-1-q) - 1 + u holds
+// Shared-memory twiddles of one tile position: entry 2^(K-1-q) + u holds
 // T[(H << (K-1-q)) + u], q = window bit.
 template <int K>
 __device__ __forceinline__ void fill_twiddles(uint64_t *tws, const DevTables &tabs, uint32_t inv, uint32_t H,
                                               uint32_t tid, uint32_t nthreads) {
-  for (uint32_t t = tid; t < (1u << K) - 1; t += nthreads) {
-    const uint32_t level = 31 - __clz(t + 1); // = K - 1 - (window bit)
-    const uint32_t u = t + 1 - (1u << level);
-    tws[t] = twiddle(tabs, inv, (H << level) + u);
+  for (uint32_t t = tid + 1; t < (1u << K); t += nthreads) {
+    const uint32_t level = 31 - __clz(t); // = K - 1 - (window bit)
+    const uint32_t u = t - (1u << level);
+    tws[tw_slot(t)] = twiddle(tabs, inv, (H << level) + u);
   }
 }
 
@@ -233,14 +266,14 @@ struct TileGeom {
 };
 
 template <int K, int C>
-__device__ __forceinline__ TileGeom tile_geom(const PassParams &p) {
+__device__ __forceinline__ TileGeom tile_geom(const PassParams &p, uint32_t bx, uint32_t by) {
   TileGeom t;
   const uint32_t lblocks_log = p.lb - LogC<C>::v;
-  const uint32_t tp = blockIdx.x;
+  const uint32_t tp = bx;
   t.H = tp >> lblocks_log;
   t.base_off = ((uint64_t)t.H << (p.lb + K)) + ((uint64_t)(tp & ((1u << lblocks_log) - 1)) << LogC<C>::v);
-  t.group = blockIdx.y / p.chunks_per_group;
-  const uint32_t chunk = blockIdx.y - t.group * p.chunks_per_group;
+  t.group = by / p.chunks_per_group;
+  const uint32_t chunk = by - t.group * p.chunks_per_group;
   t.col_begin = chunk * p.cols_per_cta;
   t.col_end = min(p.group_cols, t.col_begin + p.cols_per_cta);
   return t;
@@ -256,17 +289,19 @@ __device__ __forceinline__ void tile_elem(uint32_t e, uint32_t &g, uint64_t &off
   off = base_off + ((uint64_t)(rem / C) << lb) + rem % C;
 }
 
+// One CTA's work of a pass: tile position bx, column chunk by (blockIdx of the
+// standalone launch, or a work item of the persistent batch kernel).  Needs
+// blockDim.x == 2^log_g * 2^K * C / 16 and the shared memory of pass_smem_words.
 template <int K, int C, bool B2N>
-__global__ void __launch_bounds__(512) ntt_pass_kernel(const PassParams p) {
+__device__ __forceinline__ void pass_body(const PassParams &p, uint32_t bx, uint32_t by, uint64_t *smem) {
   constexpr int W = 1 << K;
-  extern __shared__ uint64_t smem[];
   const uint32_t G = 1u << p.log_g;
   const uint32_t TILE = G * W * C;
   const uint32_t T = TILE / 16; // == blockDim.x
   uint64_t *tile = smem;
   uint64_t *tws = smem + TILE + TILE / 16;
   const uint32_t tid = threadIdx.x;
-  const TileGeom tg = tile_geom<K, C>(p);
+  const TileGeom tg = tile_geom<K, C>(p, bx, by);
   const uint32_t Hbig = tg.H + (brev_bits(tg.group, p.log_groups) << (p.log_n - p.lb - K));
   fill_twiddles<K>(tws, p.tabs, p.inverse, Hbig, tid, T);
 
@@ -286,12 +321,12 @@ __global__ void __launch_bounds__(512) ntt_pass_kernel(const PassParams p) {
       if (col < tg.col_end) {
         const uint64_t *src = in + (uint64_t)col * p.stride_in + off;
         if (p.vec_in) {
-          const ulonglong2 v = *reinterpret_cast<const ulonglong2 *>(src);
+          const ulonglong2 v = __ldcg(reinterpret_cast<const ulonglong2 *>(src));
           v0 = v.x;
           v1 = v.y;
         } else {
-          v0 = src[0];
-          v1 = src[1];
+          v0 = __ldcg(src);
+          v1 = __ldcg(src + 1);
         }
         if (p.load_scale) {
           const uint32_t i0 = (uint32_t)off, i1 = (uint32_t)off + 1;
@@ -344,6 +379,17 @@ __global__ void __launch_bounds__(512) ntt_pass_kernel(const PassParams p) {
     }
     __syncthreads();
   }
+}
+
+// Shared memory (u64 words) of pass_body for a tile of `tile` elements.
+__host__ __device__ constexpr uint32_t pass_smem_words(uint32_t tile, int K) {
+  return tile + tile / 16 + (1u << K) + (1u << K) / 16;
+}
+
+template <int K, int C, bool B2N>
+__global__ void __launch_bounds__(256, BC_PASS_MIN_BLOCKS) ntt_pass_kernel(const PassParams p) {
+  extern __shared__ uint64_t smem[];
+  pass_body<K, C, B2N>(p, blockIdx.x, blockIdx.y, smem);
 }
 
 } // namespace bc

@@ -116,6 +116,35 @@ cudaError_t bc_lde_fused_profiled(const uint64_t *evals_bitrev, uint64_t *out, u
                                   uint32_t log_blowup, cudaStream_t stream, cudaEvent_t *events, uint32_t num_events,
                                   uint32_t *num_kernels);
 
+/* ---- uneven batches of LDE jobs in one persistent launch ------------------
+ * No counterpart in the reference, whose callers issue 1 + B batch_ntt calls
+ * per job (src/ntt.rs:179-191), each of 2-3 kernels, or log_n kernels for
+ * log_n < 16 (src/ntt.rs:201-241).  Each job is an LDE with the meaning of
+ * bc_lde_fused.  A plan schedules every job's kernels as work items of ONE
+ * persistent kernel and captures the launch in a CUDA graph; run it as often
+ * as needed (the job buffers are bound at plan time).  Plan creation
+ * allocates the schedule on the current device (records, items, counters:
+ * about 8 bytes per CTA-sized work item) and synchronises; bc_lde_batch_run
+ * is asynchronous on the stream.  The kernel's dependency waits are bounded
+ * (about 4 s each); bc_lde_batch_status returns status bit 0 if one expired,
+ * in which case that run's outputs are invalid. */
+typedef struct bc_lde_job {
+  const uint64_t *evals_bitrev;
+  uint64_t *out;
+  uint64_t stride_in, stride_out, coset_stride;
+  uint32_t log_n, num_cols, log_blowup, reserved;
+} bc_lde_job;
+
+typedef struct bc_lde_batch_plan bc_lde_batch_plan;
+
+cudaError_t bc_lde_batch_plan_create(const bc_lde_job *jobs, uint32_t n_jobs, bc_lde_batch_plan **plan);
+cudaError_t bc_lde_batch_run(bc_lde_batch_plan *plan, cudaStream_t stream);
+/* Waits for the stream, then returns the status word of the plan's last run. */
+cudaError_t bc_lde_batch_status(bc_lde_batch_plan *plan, cudaStream_t stream, uint32_t *status);
+cudaError_t bc_lde_batch_plan_info(const bc_lde_batch_plan *plan, uint32_t *n_records, uint32_t *n_items,
+                                   uint32_t *grid);
+cudaError_t bc_lde_batch_plan_destroy(bc_lde_batch_plan *plan);
+
 #ifdef __cplusplus
 }
 #endif
