@@ -56,6 +56,7 @@ SIGNATURES = {
     "bc_lde_batch_status": [_vp, _vp, _vp],
     "bc_lde_batch_plan_info": [_vp, _vp, _vp, _vp],
     "bc_lde_batch_plan_destroy": [_vp],
+    "bc_lde_batch_noalloc": [_vp, _u32, _vp, _vp],
 }
 
 

@@ -25,6 +25,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -319,3 +320,103 @@ extern "C" cudaError_t bc_lde_batch_plan_info(const bc_lde_batch_plan *plan, uin
 }
 
 extern "C" cudaError_t bc_lde_batch_plan_destroy(bc_lde_batch_plan *plan) { return free_plan(plan); }
+
+// ---------------------------------------------------------------------------
+// Batch entry point that allocates nothing.
+//
+// Some callers cannot call cudaMalloc: a prover that reserves nearly all of
+// HBM for its own memory pool at start-up and sub-allocates from it (a
+// cudaMalloc then fails or fragments the pool), or a latency-critical
+// submission path where the implicit device-wide synchronisation of
+// cudaMalloc/cudaFree would stall work on other streams.  For them the
+// batch schedule (records, work items, counters) lives in the fixed array
+// below instead of plan-owned allocations.  The array is part of this
+// library's device image, so every GPU that loads the library holds its
+// 16 MiB until the process exits.
+namespace bc {
+constexpr size_t NOALLOC_SCRATCH_BYTES = 16u << 20;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
+
+namespace {
+constexpr int NOALLOC_MAX_DEVICES = 64;
+void *g_noalloc_base[NOALLOC_MAX_DEVICES] = {};
+int g_noalloc_grid[NOALLOC_MAX_DEVICES] = {};
+std::mutex g_noalloc_mutex;
+
+// First call on a device: device address of the scratch array and the
+// persistent grid size.  Host code cannot use g_noalloc_scratch directly --
+// in host code that name is only a stand-in for the device symbol.
+cudaError_t noalloc_setup(int dev, void **base, int *grid) {
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_base[dev]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(lde_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)BATCH_SMEM_BYTES);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lde_batch_kernel, BATCH_THREADS, BATCH_SMEM_BYTES);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    g_noalloc_grid[dev] = per_sm * sm_count();
+    g_noalloc_base[dev] = p;
+  }
+  *base = g_noalloc_base[dev];
+  *grid = g_noalloc_grid[dev];
+  return cudaSuccess;
+}
+
+size_t round256(size_t x) { return (x + 255) & ~(size_t)255; }
+} // namespace
+} // namespace bc
+
+extern "C" cudaError_t bc_lde_batch_noalloc(const bc_lde_job *jobs, uint32_t n_jobs, cudaStream_t stream,
+                                            uint32_t *status) {
+  if (n_jobs && !jobs) return cudaErrorInvalidValue;
+  if (!device_tables()) return cudaErrorInitializationError;
+  const int dev = current_device();
+  if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return cudaErrorInvalidDevice;
+  void *base = nullptr;
+  int grid = 0;
+  cudaError_t e = noalloc_setup(dev, &base, &grid);
+  if (e != cudaSuccess) return e;
+  std::vector<BatchRecord> recs;
+  std::vector<uint64_t> items;
+  e = schedule(jobs, n_jobs, recs, items);
+  if (e != cudaSuccess) return e;
+  // layout: counters (done[n_records], next, status) | records | items
+  const size_t counters_bytes = round256((recs.size() + 2) * sizeof(uint32_t));
+  const size_t recs_bytes = round256(recs.size() * sizeof(BatchRecord));
+  const size_t items_bytes = items.size() * sizeof(uint64_t);
+  if (counters_bytes + recs_bytes + items_bytes > NOALLOC_SCRATCH_BYTES) return cudaErrorInvalidValue;
+  unsigned char *b = static_cast<unsigned char *>(base);
+  uint32_t *counters = reinterpret_cast<uint32_t *>(b);
+  BatchRecord *d_recs = reinterpret_cast<BatchRecord *>(b + counters_bytes);
+  uint64_t *d_items = reinterpret_cast<uint64_t *>(b + counters_bytes + recs_bytes);
+  // the previous call's contents stay in the array: the counters must start at zero
+  e = cudaMemsetAsync(counters, 0, (recs.size() + 2) * sizeof(uint32_t), stream);
+  if (e != cudaSuccess) return e;
+  if (!items.empty()) {
+    // pageable sources: each copy has consumed its host buffer when it returns
+    e = cudaMemcpyAsync(d_recs, recs.data(), recs.size() * sizeof(BatchRecord), cudaMemcpyHostToDevice, stream);
+    if (e != cudaSuccess) return e;
+    e = cudaMemcpyAsync(d_items, items.data(), items_bytes, cudaMemcpyHostToDevice, stream);
+    if (e != cudaSuccess) return e;
+    int clock_khz = 0;
+    cudaDeviceGetAttribute(&clock_khz, cudaDevAttrClockRate, dev);
+    const long long timeout = (long long)std::max(clock_khz, 1000000) * 1000ll * 4;
+    const uint32_t n_rec = (uint32_t)recs.size();
+    lde_batch_kernel<<<grid, BATCH_THREADS, BATCH_SMEM_BYTES, stream>>>(d_recs, d_items, (uint32_t)items.size(),
+                                                                         counters, counters + n_rec,
+                                                                         counters + n_rec + 1, timeout);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  if (status) {
+    *status = 0;
+    e = cudaMemcpyAsync(status, counters + recs.size() + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream);
+    if (e != cudaSuccess) return e;
+    e = cudaStreamSynchronize(stream);
+  }
+  return e;
+}

@@ -145,6 +145,24 @@ cudaError_t bc_lde_batch_plan_info(const bc_lde_batch_plan *plan, uint32_t *n_re
                                    uint32_t *grid);
 cudaError_t bc_lde_batch_plan_destroy(bc_lde_batch_plan *plan);
 
+/* No counterpart in the reference.  The same batch as a plan, run once, for
+ * callers that cannot allocate device memory -- for example a prover that has
+ * reserved nearly all of HBM for its own pool at start-up, or a
+ * latency-critical submission path that cannot afford the device-wide
+ * synchronisation of cudaMalloc/cudaFree.  It calls no cudaMalloc or
+ * cudaFree: the schedule goes into a fixed 16 MiB array inside this library,
+ * which every GPU that loads the library holds until the process exits.  A
+ * batch whose schedule does not fit (about two million 4096-element work
+ * items) returns cudaErrorInvalidValue.  The first call on a device looks up
+ * the array's device address and the kernel's occupancy; make that first call
+ * before any stream capture.  All calls on a device share the array: calls
+ * whose work overlaps on the GPU (different streams, not ordered by events)
+ * race and corrupt each other; calls ordered on one stream are safe.
+ * status (optional): if non-null, the call waits for the stream and stores
+ * the batch status word (bit 0: a bounded dependency wait expired and the
+ * outputs are invalid). */
+cudaError_t bc_lde_batch_noalloc(const bc_lde_job *jobs, uint32_t n_jobs, cudaStream_t stream, uint32_t *status);
+
 #ifdef __cplusplus
 }
 #endif
