@@ -252,6 +252,86 @@ __device__ __forceinline__ void fill_twiddles(uint64_t *tws, const DevTables &ta
   }
 }
 
+// ---------------------------------------------------------------- full rounds at a runtime bit offset
+// A full round holds 4 window bits [B, B + 4) of one group per thread.  The
+// network below is written once per direction and reused for every full
+// round of a pass (looped with `#pragma unroll 1`), which keeps a kernel to one
+// copy of the 32-butterfly register network instead of one per round.
+
+// Tile index of element 0 of group gi (runs of C fastest) and its window value w.
+template <int K, int C>
+__device__ __forceinline__ uint32_t gbase16(uint32_t gi, uint32_t B, uint32_t &w) {
+  const uint32_t lc = gi % C;
+  const uint32_t rest = gi / C;
+  const uint32_t g = rest >> (K - 4);
+  const uint32_t wo = rest & ((1u << (K - 4)) - 1);
+  w = (wo & ((1u << B) - 1)) | ((wo >> B) << (B + 4));
+  return ((g << K) | w) * C + lc;
+}
+
+// Padded tile slots of the 16 elements of a group: element j sits at tile
+// index eb + j * S, S = C << B.
+__device__ __forceinline__ void slots16(uint32_t eb, uint32_t S, uint32_t (&a)[16]) {
+  if (S >= 16) { // S is a multiple of 16: the padding advances by S / 16 per element
+    const uint32_t p0 = pad16(eb), s17 = S + (S >> 4);
+#pragma unroll
+    for (int j = 0; j < 16; j++) a[j] = p0 + (uint32_t)j * s17;
+  } else {
+#pragma unroll
+    for (int j = 0; j < 16; j++) a[j] = pad16(eb + (uint32_t)j * S);
+  }
+}
+
+// The four stages of a full round on x[16] (element j at window w | j << B).
+// The twiddle of stage bit qb for element pair j0 is entry
+// 2^(K-1-qb) + (w >> (qb+1)) + (j0 >> (qq+1)) of the tile's table; the last
+// term never carries across a pad word, so one base pointer per stage serves
+// all its pairs with constant offsets.
+template <int K, bool DIF>
+__device__ __forceinline__ void net16(uint64_t (&x)[16], const uint64_t *tws, uint32_t w, uint32_t B) {
+  const uint64_t *tp[4];
+#pragma unroll
+  for (int qq = 0; qq < 4; qq++) {
+    const uint32_t qb = B + qq;
+    tp[qq] = tws + tw_slot((1u << (K - 1 - qb)) + (w >> (qb + 1)));
+  }
+#pragma unroll
+  for (int st = 0; st < 4; st++) {
+    const int qq = DIF ? st : 3 - st;
+#pragma unroll
+    for (int j0 = 0; j0 < 16; j0++) {
+      if (j0 & (1 << qq)) continue;
+      const uint64_t t = tp[qq][j0 >> (qq + 1)];
+      if (DIF)
+        dif(x[j0], x[j0 | (1 << qq)], t);
+      else
+        dit(x[j0], x[j0 | (1 << qq)], t);
+    }
+  }
+}
+
+// Full rounds at bit offsets B0, B0 + dB, ... (count rounds) through shared
+// memory, each followed by a barrier.  One thread per group.
+template <int K, int C, bool DIF>
+__device__ __forceinline__ void full_rounds(uint64_t *tile, const uint64_t *tws, int B0, int dB, int count,
+                                            uint32_t tid) {
+#pragma unroll 1
+  for (int r = 0; r < count; r++) {
+    const uint32_t B = (uint32_t)(B0 + r * dB);
+    uint32_t w;
+    const uint32_t eb = gbase16<K, C>(tid, B, w);
+    uint32_t a[16];
+    slots16(eb, (uint32_t)C << B, a);
+    uint64_t x[16];
+#pragma unroll
+    for (int j = 0; j < 16; j++) x[j] = tile[a[j]];
+    net16<K, DIF>(x, tws, w, B);
+#pragma unroll
+    for (int j = 0; j < 16; j++) tile[a[j]] = x[j];
+    __syncthreads();
+  }
+}
+
 template <int C> struct LogC {
   static constexpr int v = C == 1 ? 0 : C == 2 ? 1 : C == 4 ? 2 : 3;
 };
@@ -292,9 +372,19 @@ __device__ __forceinline__ void tile_elem(uint32_t e, uint32_t &g, uint64_t &off
 // One CTA's work of a pass: tile position bx, column chunk by (blockIdx of the
 // standalone launch, or a work item of the persistent batch kernel).  Needs
 // blockDim.x == 2^log_g * 2^K * C / 16 and the shared memory of pass_smem_words.
+//
+// Round order.  Natural->bit-reversed: the first full round (top 4 window
+// bits) is loaded straight from global memory into registers (consecutive
+// threads read consecutive addresses), the remaining full rounds run from the
+// top down through shared memory, the short round (K mod 4 bits at the bottom)
+// last, then the tile is stored with 16-byte stores.  Bit-reversed->natural:
+// the tile is loaded with 16-byte loads, the short round runs first at the
+// bottom, the full rounds upwards, and the last full round (top 4 bits) is
+// stored straight from registers.
 template <int K, int C, bool B2N>
 __device__ __forceinline__ void pass_body(const PassParams &p, uint32_t bx, uint32_t by, uint64_t *smem) {
   constexpr int W = 1 << K;
+  constexpr int R = K % 4, NF = K / 4;
   const uint32_t G = 1u << p.log_g;
   const uint32_t TILE = G * W * C;
   const uint32_t T = TILE / 16; // == blockDim.x
@@ -309,39 +399,116 @@ __device__ __forceinline__ void pass_body(const PassParams &p, uint32_t bx, uint
   uint64_t *out = p.out + tg.group * p.group_stride_out;
   const uint32_t mask_n = (1u << p.log_n) - 1;
 
-  for (uint32_t c0 = tg.col_begin; c0 < tg.col_end; c0 += G) {
-#pragma unroll
-    for (int j = 0; j < 8; j++) {
-      const uint32_t e = 2 * (tid + T * j);
-      uint32_t g;
-      uint64_t off;
-      tile_elem<K, C>(e, g, off, tg.base_off, p.lb);
-      const uint32_t col = c0 + g;
-      uint64_t v0 = 0, v1 = 0;
-      if (col < tg.col_end) {
-        const uint64_t *src = in + (uint64_t)col * p.stride_in + off;
-        if (p.vec_in) {
-          const ulonglong2 v = __ldcg(reinterpret_cast<const ulonglong2 *>(src));
-          v0 = v.x;
-          v1 = v.y;
-        } else {
-          v0 = __ldcg(src);
-          v1 = __ldcg(src + 1);
-        }
-        if (p.load_scale) {
-          const uint32_t i0 = (uint32_t)off, i1 = (uint32_t)off + 1;
-          const uint32_t n0 = B2N ? brev_bits(i0, p.log_n) : i0;
-          const uint32_t n1 = B2N ? brev_bits(i1 & mask_n, p.log_n) : i1;
-          v0 = gl::mul(v0, coset_power(p.tabs, 0, n0, p.coset_kshift));
-          v1 = gl::mul(v1, coset_power(p.tabs, 0, n1, p.coset_kshift));
-        }
-      }
-      tile[pad16(e)] = v0;
-      tile[pad16(e) + 1] = v1;
-    }
-    __syncthreads();
+  // global offset (within the column) and column of element 0 of a full-round group
+  auto group_origin = [&](uint32_t eb, uint32_t c0, uint64_t &off0, uint32_t &col) {
+    uint32_t g;
+    tile_elem<K, C>(eb, g, off0, tg.base_off, p.lb);
+    col = c0 + g;
+  };
 
-    rounds_from<K, C, B2N, false, 0>(tile, tws, tid, T);
+  for (uint32_t c0 = tg.col_begin; c0 < tg.col_end; c0 += G) {
+    if constexpr (!B2N && NF > 0) {
+      __syncthreads(); // twiddles ready; previous column group's stores done
+      // first full round straight from global memory
+      constexpr uint32_t B = K - 4;
+      uint32_t w;
+      const uint32_t eb = gbase16<K, C>(tid, B, w);
+      uint64_t off0;
+      uint32_t col;
+      group_origin(eb, c0, off0, col);
+      uint64_t x[16];
+      if (col < tg.col_end) {
+        const uint64_t *src = in + (uint64_t)col * p.stride_in + off0;
+        const uint64_t step = 1ull << (B + p.lb);
+#pragma unroll
+        for (int j = 0; j < 16; j++) x[j] = __ldcg(src + j * step);
+        if (p.load_scale) {
+#pragma unroll
+          for (int j = 0; j < 16; j++)
+            x[j] = gl::mul(x[j], coset_power(p.tabs, 0, (uint32_t)(off0 + j * step), p.coset_kshift));
+        }
+      } else {
+#pragma unroll
+        for (int j = 0; j < 16; j++) x[j] = 0;
+      }
+      net16<K, false>(x, tws, w, B);
+      uint32_t a[16];
+      slots16(eb, (uint32_t)C << B, a);
+#pragma unroll
+      for (int j = 0; j < 16; j++) tile[a[j]] = x[j];
+      __syncthreads();
+      full_rounds<K, C, false>(tile, tws, (int)B - 4, -4, NF - 1, tid);
+      if constexpr (R > 0) rounds_from<K, C, false, false, NF>(tile, tws, tid, T);
+    } else {
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        const uint32_t e = 2 * (tid + T * j);
+        uint32_t g;
+        uint64_t off;
+        tile_elem<K, C>(e, g, off, tg.base_off, p.lb);
+        const uint32_t col = c0 + g;
+        uint64_t v0 = 0, v1 = 0;
+        if (col < tg.col_end) {
+          const uint64_t *src = in + (uint64_t)col * p.stride_in + off;
+          if (p.vec_in) {
+            const ulonglong2 v = __ldcg(reinterpret_cast<const ulonglong2 *>(src));
+            v0 = v.x;
+            v1 = v.y;
+          } else {
+            v0 = __ldcg(src);
+            v1 = __ldcg(src + 1);
+          }
+          if (p.load_scale) {
+            const uint32_t i0 = (uint32_t)off, i1 = (uint32_t)off + 1;
+            const uint32_t n0 = B2N ? brev_bits(i0, p.log_n) : i0;
+            const uint32_t n1 = B2N ? brev_bits(i1 & mask_n, p.log_n) : i1;
+            v0 = gl::mul(v0, coset_power(p.tabs, 0, n0, p.coset_kshift));
+            v1 = gl::mul(v1, coset_power(p.tabs, 0, n1, p.coset_kshift));
+          }
+        }
+        tile[pad16(e)] = v0;
+        tile[pad16(e) + 1] = v1;
+      }
+      __syncthreads();
+      if constexpr (!B2N) {
+        rounds_from<K, C, false, false, 0>(tile, tws, tid, T); // K < 4: one short round
+      } else if constexpr (NF == 0) {
+        rounds_from<K, C, true, true, 0>(tile, tws, tid, T);
+      } else {
+        if constexpr (R > 0) rounds_from<K, C, true, true, 0, 1>(tile, tws, tid, T);
+        full_rounds<K, C, true>(tile, tws, R, 4, NF - 1, tid);
+        // last full round (top 4 bits) stored straight from registers
+        constexpr uint32_t B = K - 4;
+        uint32_t w;
+        const uint32_t eb = gbase16<K, C>(tid, B, w);
+        uint32_t a[16];
+        slots16(eb, (uint32_t)C << B, a);
+        uint64_t x[16];
+#pragma unroll
+        for (int j = 0; j < 16; j++) x[j] = tile[a[j]];
+        net16<K, true>(x, tws, w, B);
+        uint64_t off0;
+        uint32_t col;
+        group_origin(eb, c0, off0, col);
+        if (col < tg.col_end) {
+          uint64_t *dst = out + (uint64_t)col * p.stride_out + off0;
+          const uint64_t step = 1ull << (B + p.lb);
+          const uint64_t s = p.tabs.inv_pow2[p.log_n];
+#pragma unroll
+          for (int j = 0; j < 16; j++) {
+            uint64_t v = x[j];
+            if (p.store_scale) {
+              const uint32_t i = (uint32_t)(off0 + j * step); // natural index of a bit-reversed->natural output
+              v = gl::mul(v, p.has_coset ? gl::mul(s, coset_power(p.tabs, 1, i, p.coset_kshift)) : s);
+            }
+            if (p.canon_out) v = gl::canon(v);
+            __stcg(dst + j * step, v);
+          }
+        }
+        __syncthreads();
+        continue;
+      }
+    }
 
 #pragma unroll
     for (int j = 0; j < 8; j++) {
