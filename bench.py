@@ -283,21 +283,26 @@ def run_ours(args, rank, world):
                     "traffic": None, "kernel_ms": [round(v, 3) for v in kern_ms],
                     "step_algorithmic_frac": round(8 * n * COLS * (1 + B) / (ms_per_step / 1e3) / 1e9 / peak, 4)}
 
-    # end to end through the C ABI with host buffers: pinned H2D, LDE, D2H every step
+    # end to end through the C ABI with host buffers: bc_lde_host takes pinned host input and writes pinned
+    # host output every step, overlapping chunked copy-in / transform / copy-out on three streams
     hx = torch.empty(COLS * n, dtype=torch.int64, pin_memory=True)
     hx.copy_(x)
     hout = torch.empty(B * COLS * n, dtype=torch.int64, pin_memory=True)
-    dx = torch.empty_like(x)
+    chunk_cols = max(1, min(COLS, 8))
+    ws = torch.empty(3 * chunk_cols * n * (1 + B), dtype=torch.int64, device="cuda")
 
     def e2e_step():
-        dx.copy_(hx, non_blocking=True)
-        rc = L.bc_lde_fused(dx.data_ptr(), op, LOG_N, COLS, n, n, COLS * n, LOG_BLOWUP, s_handle)
-        assert rc == 0
-        hout.copy_(out, non_blocking=True)
+        rc = L.bc_lde_host(hx.data_ptr(), hout.data_ptr(), LOG_N, COLS, n, n, COLS * n, LOG_BLOWUP, ws.data_ptr(),
+                           ws.numel() * 8, chunk_cols, s_handle)
+        assert rc == 0, rc
 
     e2e_steps = max(2, min(args.steps, 5))
     e2e_ms, _ = time_steps(e2e_step, e2e_steps, 1, world, stream)
     e2e_value = world * e2e_steps * out_elems / (e2e_ms / 1e3) / 1e6
+    # the result must be the device LDE's, bit for bit (checked on the last step's host output)
+    fused()
+    torch.cuda.synchronize()
+    e2e_exact = bool(torch.equal(hout, out.cpu())) if COLS * n <= (1 << 30) else None
 
     line = {
         "metric": METRIC, "value": round(value, 1), "unit": "Melem/s", "n_gpus": world, "steps": args.steps,
@@ -314,12 +319,126 @@ def run_ours(args, rank, world):
         "clocks": clk.summary(),
         "e2e": {"value": round(e2e_value, 1), "unit": "Melem/s", "h2d_bytes_per_step": 8 * COLS * n,
                 "d2h_bytes_per_step": 8 * B * COLS * n, "ms_per_step": round(e2e_ms / e2e_steps, 3),
-                "path": "pinned host -> bc_lde_fused -> pinned host, one stream"},
+                "path": f"bc_lde_host: pinned host in/out, {chunk_cols}-column chunks, copies overlapped",
+                "bit_exact_vs_device": e2e_exact},
         "gpu_launches": args.steps * (len(kern_ms) if kern_ms else 3),
     }
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(os.cpu_count() or 1)
+    del x, out, hx, hout, ws
+    torch.cuda.empty_cache()
+    if world == 1 and not args.no_batch:
+        line["batch"] = run_batch_section()
+    if world == 1 and not args.no_serve:
+        line["serve"] = run_serve_section()
     return line
+
+
+def _uneven_tensors(specs):
+    import torch
+
+    tens = []
+    for sp in specs:
+        g = torch.Generator(device="cuda").manual_seed(sp.seed)
+        ev = torch.randint(-(2**63), 2**63 - 1, (sp.in_words,), device="cuda", dtype=torch.int64, generator=g)
+        ev = torch.where((ev < 0) & (ev >= -(2**32 - 1)), ev + (2**32 - 1), ev)  # uniform in [0, p)
+        tens.append((ev, torch.empty(sp.out_words, dtype=torch.int64, device="cuda"), sp.log_n, sp.cols,
+                     sp.log_blowup))
+    return tens
+
+
+def run_batch_section(reps: int = 3):
+    """96 seeded uneven LDE jobs: one persistent launch vs one call per job (fused, plain)."""
+    import torch
+
+    import bc_ntt
+    import workloads
+
+    specs = workloads.uneven_batch(n_jobs=96, seed=42)
+    tens = _uneven_tensors(specs)
+    plan = bc_ntt.LdeBatch(tens)
+    stream = torch.cuda.current_stream()
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    out_elems = sum(sp.out_words for sp in specs)
+    t_batch = timed(plan.run)
+    status = plan.status()
+    batch_out = [t[1].clone() for t in tens[:8]]
+    t_fused = timed(lambda: [bc_ntt.lde(*t, fused=True) for t in tens])
+    exact = all(torch.equal(a, t[1]) for a, t in zip(batch_out, tens[:8]))
+    t_plain = timed(lambda: [bc_ntt.lde(*t, fused=False) for t in tens])
+    info = plan.info()
+    plan.close()
+    del tens, batch_out
+    torch.cuda.empty_cache()
+    mel = lambda ms: round(out_elems / (ms / 1e3) / 1e6, 1)  # noqa: E731
+    return {"workload": "96 jobs, log_n U{12..22}, cols log-U[1,256], blowup U{2,4,8}, seed 42",
+            "total_out_gelem": round(out_elems / 1e9, 2),
+            "persistent_one_launch": {"ms": round(t_batch, 2), "value": mel(t_batch), "status": status,
+                                      "records": info["records"], "items": info["items"], "grid": info["grid"]},
+            "per_job_fused": {"ms": round(t_fused, 2), "value": mel(t_fused)},
+            "per_job_plain": {"ms": round(t_plain, 2), "value": mel(t_plain)},
+            "persistent_vs_plain": round(t_plain / t_batch, 3), "fused_vs_plain": round(t_plain / t_fused, 3),
+            "bit_exact_persistent_vs_per_job": bool(exact), "unit": "Melem/s"}
+
+
+def run_serve_section(n_requests: int = 48, rate: float = 20.0, budget_gib: int = 40, slots: int = 4):
+    """Poisson LDE requests through the continuous-batching server vs the same requests served one at a time."""
+    import torch
+
+    import bc_ntt
+    import workloads
+
+    reqs = workloads.serving_stream(n_requests=n_requests, rate_per_s=rate, seed=7)
+    max_in = max(r.in_words for r in reqs)
+    max_out = max(r.out_words for r in reqs)
+    # host pools reused by every request (timing; per-request exactness is covered by tests/test_server_gpu.py)
+    hin = torch.randint(0, 2**62, (max_in,), dtype=torch.int64).pin_memory()
+    hout = torch.empty(max_out, dtype=torch.int64).pin_memory()
+    srv = bc_ntt.LdeServer(memory_budget_bytes=budget_gib << 30, slots=slots)
+    t0 = time.perf_counter()
+    ids = []
+    for r in reqs:
+        d = t0 + r.arrival_s - time.perf_counter()
+        if d > 0:
+            time.sleep(d)
+        ids.append(srv.submit(hin, hout, r.log_n, r.cols, r.log_blowup))
+    for i in ids:
+        srv.wait(i, timeout_ms=600000)
+    wall = time.perf_counter() - t0
+    st = srv.stats()
+    srv.close()
+    # the same requests, one at a time through the plain path (copy in, bc_lde_plain, copy out)
+    dev_in = torch.empty(max_in, dtype=torch.int64, device="cuda")
+    dev_out = torch.empty(max_out, dtype=torch.int64, device="cuda")
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    for r in reqs:
+        dev_in[:r.in_words].copy_(hin[:r.in_words], non_blocking=True)
+        bc_ntt.lde(dev_in, dev_out, r.log_n, r.cols, r.log_blowup, fused=False)
+        hout[:r.out_words].copy_(dev_out[:r.out_words], non_blocking=True)
+    torch.cuda.synchronize()
+    serial = time.perf_counter() - t1
+    out_elems = sum(r.out_words for r in reqs)
+    del dev_in, dev_out, hin, hout
+    torch.cuda.empty_cache()
+    return {"workload": f"{n_requests} Poisson requests at {rate}/s, log_n U{{14..22}}, cols log-U[8,512], "
+                        f"blowup U{{2,4}}, seed 7, host buffers (pinned)",
+            "budget_gib": budget_gib, "slots": slots, "p50_ms": round(st["p50_ms"], 2), "p99_ms": round(st["p99_ms"], 2),
+            "max_ms": round(st["max_ms"], 2), "value": round(st["out_melem_per_s"], 1),
+            "wall_s": round(wall, 3), "serial_plain_s": round(serial, 3),
+            "serial_plain_value": round(out_elems / serial / 1e6, 1), "unit": "Melem/s",
+            "completed": st["completed"]}
 
 
 def run_reference(args, rank, world):
@@ -385,6 +504,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-batch", action="store_true", help="skip the uneven-batch section")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving section")
     ap.add_argument("--log-n", type=int, default=22, help="column length 2^log_n (default 22)")
     ap.add_argument("--cols", type=int, default=128, help="columns (default 128)")
     ap.add_argument("--log-blowup", type=int, default=1, help="log2 of the blowup (default 1)")

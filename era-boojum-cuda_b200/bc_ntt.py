@@ -51,13 +51,34 @@ SIGNATURES = {
     "bc_lde_plain": [_vp, _vp, _u32, _u32, _u64, _u64, _u64, _u32, _vp],
     "bc_lde_fused": [_vp, _vp, _u32, _u32, _u64, _u64, _u64, _u32, _vp],
     "bc_lde_fused_profiled": [_vp, _vp, _u32, _u32, _u64, _u64, _u64, _u32, _vp, _vp, _u32, _vp],
+    "bc_lde_host": [_vp, _vp, _u32, _u32, _u64, _u64, _u64, _u32, _vp, _sz, _u32, _vp],
     "bc_lde_batch_plan_create": [_vp, _u32, _vp],
     "bc_lde_batch_run": [_vp, _vp],
     "bc_lde_batch_status": [_vp, _vp, _vp],
     "bc_lde_batch_plan_info": [_vp, _vp, _vp, _vp],
     "bc_lde_batch_plan_destroy": [_vp],
     "bc_lde_batch_noalloc": [_vp, _u32, _vp, _vp],
+    "bc_lde_server_create": [_vp, _vp],
+    "bc_lde_server_submit": [_vp, _vp, _vp, _u32, _u32, _u32, _vp],
+    "bc_lde_server_poll": [_vp, _u64, _vp, _vp],
+    "bc_lde_server_wait": [_vp, _u64, _u32, _vp],
+    "bc_lde_server_cancel": [_vp, _u64],
+    "bc_lde_server_get_stats": [_vp, _vp],
+    "bc_lde_server_destroy": [_vp],
 }
+
+CUDA_ERROR_NOT_READY = 600
+CUDA_ERROR_TIMEOUT = 909
+
+
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("memory_budget_bytes", _sz), ("slots", _u32), ("max_chunk_cols", _u32)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("completed", _u64), ("pending", _u64), ("running", _u64), ("p50_ms", ctypes.c_double),
+                ("p99_ms", ctypes.c_double), ("max_ms", ctypes.c_double), ("span_s", ctypes.c_double),
+                ("out_melem_per_s", ctypes.c_double), ("arena_largest_free", _sz)]
 
 
 class LdeJob(ctypes.Structure):
@@ -222,3 +243,65 @@ class LdeBatch:
             self.close()
         except Exception:
             pass
+
+
+def lde_host(host_evals, host_out, log_n: int, num_cols: int, log_blowup: int, workspace, max_chunk_cols: int = 0,
+             stream=None):
+    """LDE from host tensors (pinned for overlap) to host tensors through a device workspace tensor."""
+    n = 1 << log_n
+    _check(lib().bc_lde_host(_ptr(host_evals), _ptr(host_out), log_n, num_cols, n, n, num_cols * n, log_blowup,
+                             _ptr(workspace), workspace.numel() * workspace.element_size(), max_chunk_cols,
+                             _stream(stream)), "lde_host")
+
+
+class LdeServer:
+    """Continuous-batching LDE server (bc_lde_server_*) on the current device."""
+
+    PENDING, RUNNING, DONE, CANCELLED, FAILED = range(5)
+
+    def __init__(self, memory_budget_bytes: int, slots: int = 4, max_chunk_cols: int = 0):
+        cfg = ServerConfig(memory_budget_bytes, slots, max_chunk_cols)
+        self.handle = ctypes.c_void_p()
+        _check(lib().bc_lde_server_create(ctypes.byref(cfg), ctypes.byref(self.handle)), "bc_lde_server_create")
+        self._keep = {}
+
+    def submit(self, host_evals, host_out, log_n: int, num_cols: int, log_blowup: int) -> int:
+        rid = ctypes.c_uint64()
+        _check(lib().bc_lde_server_submit(self.handle, _ptr(host_evals), _ptr(host_out), log_n, num_cols, log_blowup,
+                                          ctypes.byref(rid)), "bc_lde_server_submit")
+        self._keep[rid.value] = (host_evals, host_out)
+        return rid.value
+
+    def poll(self, rid: int):
+        st, lat = ctypes.c_int(), ctypes.c_double()
+        _check(lib().bc_lde_server_poll(self.handle, rid, ctypes.byref(st), ctypes.byref(lat)), "poll")
+        return st.value, lat.value
+
+    def wait(self, rid: int, timeout_ms: int = 60000) -> float:
+        """Latency in ms; raises TimeoutError / RuntimeError (cancelled or failed)."""
+        lat = ctypes.c_double()
+        rc = lib().bc_lde_server_wait(self.handle, rid, timeout_ms, ctypes.byref(lat))
+        if rc == CUDA_ERROR_TIMEOUT:
+            raise TimeoutError(f"request {rid} not finished after {timeout_ms} ms")
+        if rc == CUDA_ERROR_NOT_READY:
+            raise RuntimeError(f"request {rid} was cancelled")
+        _check(rc, "bc_lde_server_wait")
+        return lat.value
+
+    def cancel(self, rid: int) -> bool:
+        rc = lib().bc_lde_server_cancel(self.handle, rid)
+        if rc == CUDA_ERROR_NOT_READY:
+            return False
+        _check(rc, "bc_lde_server_cancel")
+        return True
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _check(lib().bc_lde_server_get_stats(self.handle, ctypes.byref(st)), "bc_lde_server_get_stats")
+        return {f: getattr(st, f) for f, _ in ServerStats._fields_}
+
+    def close(self):
+        if self.handle:
+            _check(lib().bc_lde_server_destroy(self.handle), "bc_lde_server_destroy")
+            self.handle = ctypes.c_void_p()
+            self._keep.clear()

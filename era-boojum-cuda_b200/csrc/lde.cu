@@ -218,11 +218,9 @@ cudaError_t launch_lde_step(const LdeStep &st, cudaStream_t stream) {
   return cudaGetLastError();
 }
 
-// events (optional): ev[0] is recorded before the first kernel and ev[j + 1]
-// after kernel j, for as many events as are given.
 cudaError_t lde_fused(const Plan &pl, const uint64_t *in, uint64_t *out, uint32_t log_n, uint32_t num_cols,
                       uint64_t stride_in, uint64_t stride_out, uint64_t coset_stride, uint32_t log_blowup,
-                      cudaStream_t stream, cudaEvent_t *ev = nullptr, uint32_t n_ev = 0) {
+                      cudaStream_t stream, cudaEvent_t *ev, uint32_t n_ev) {
   if (!device_tables()) return cudaErrorInitializationError;
   if (num_cols == 0) return cudaSuccess;
   std::vector<LdeStep> steps;

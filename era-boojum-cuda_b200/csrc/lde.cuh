@@ -30,15 +30,41 @@ struct LdeTopParams {
   DevTables tabs;
 };
 
+// Stores coset k of the tile (16-byte stores; canonical when this kernel ends the LDE).
+template <int K, int C>
+__device__ __forceinline__ void top_store_t(const LdeTopParams &p, const uint64_t *tile, uint32_t c0, uint32_t col_end,
+                                            uint32_t k, uint64_t base_off, uint32_t tid, uint32_t T) {
+  uint64_t *out = p.out + (uint64_t)k * p.coset_stride;
+#pragma unroll
+  for (int j = 0; j < 8; j++) {
+    const uint32_t e = 2 * (tid + T * j);
+    uint32_t g;
+    uint64_t off;
+    tile_elem<K, C>(e, g, off, base_off, p.lb);
+    const uint32_t col = c0 + g;
+    if (col >= col_end) continue;
+    uint64_t v0 = tile[pad16(e)], v1 = tile[pad16(e) + 1];
+    if (p.canon_out) {
+      v0 = gl::canon(v0);
+      v1 = gl::canon(v1);
+    }
+    uint64_t *dst = out + (uint64_t)col * p.stride_out + off;
+    if (p.vec_out) {
+      *reinterpret_cast<ulonglong2 *>(dst) = make_ulonglong2(v0, v1);
+    } else {
+      dst[0] = v0;
+      dst[1] = v1;
+    }
+  }
+}
+#define top_store top_store_t<K, C>
+
 // One CTA's work of the top-window kernel: tile position bx (run of low
 // positions), column chunk by.  blockDim.x == 2^log_g * 2^K * C / 16.
 template <int K, int C>
 __device__ __forceinline__ void top_body(const LdeTopParams &p, uint32_t bx, uint32_t by, uint64_t *smem) {
   constexpr int W = 1 << K;
-  using LastInv = RoundShape<K, true, true, (K + 3) / 4 - 1>; // last inverse round ...
-  using FirstFwd = RoundShape<K, false, false, 0>;            // ... holds the first forward round's groups
-  static_assert(LastInv::B == FirstFwd::B && LastInv::V == FirstFwd::V, "round hand-over mismatch");
-  constexpr int BB = FirstFwd::B, VV = FirstFwd::V, NV = 1 << VV, NG = 16 / NV;
+  constexpr int R = K % 4, NF = K / 4;
   const uint32_t G = 1u << p.log_g;
   const uint32_t TILE = G * W * C;
   const uint32_t T = TILE / 16;
@@ -53,8 +79,6 @@ __device__ __forceinline__ void top_body(const LdeTopParams &p, uint32_t bx, uin
   const uint32_t col_end = min(p.num_cols, col_begin + p.cols_per_cta);
   fill_twiddles<K>(tws_inv, p.tabs, 1, 0, tid, T);
 
-  // scale n^-1 g^i of this thread's groups: i = base + lc + (w_j << lb), w_j = w | (j << BB)
-  const uint64_t g_step = g_power(p.tabs, 0, 1u << (p.lb + BB));
   const uint64_t inv_n = p.tabs.inv_pow2[p.log_n];
   const uint32_t nb = 1u << p.log_blowup;
 
@@ -83,57 +107,104 @@ __device__ __forceinline__ void top_body(const LdeTopParams &p, uint32_t bx, uin
     }
     __syncthreads();
 
-    // inverse stages of the window (bottom-up), all but the last round through shared memory
-    rounds_from<K, C, true, true, 0, (K + 3) / 4 - 1>(tile, tws_inv, tid, T);
-    uint64_t coef[16];
-    load_groups<K, C, BB, VV>(tile, coef, tid, T);
-    compute_groups<K, C, true, BB, VV>(coef, tws_inv, tid, T);
+    if constexpr (NF == 0) {
+      // window of fewer than 4 bits: one short round each way, in registers
+      using S = RoundShape<K, false, false, 0>;
+      uint64_t coef[16];
+      load_groups<K, C, S::B, S::V>(tile, coef, tid, T);
+      compute_groups<K, C, true, S::B, S::V>(coef, tws_inv, tid, T);
+      constexpr int NV = 1 << S::V, NG = 16 / NV;
 #pragma unroll
-    for (int q = 0; q < NG; q++) {
-      uint32_t w;
-      const uint32_t gi = tid + T * q;
-      group_base<K, C, BB, VV>(gi, w);
-      const uint32_t i0 = (uint32_t)base_off + gi % C + (w << p.lb);
-      uint64_t s = gl::mul(inv_n, g_power(p.tabs, 0, i0));
+      for (int q = 0; q < NG; q++) {
+        uint32_t w;
+        const uint32_t gi = tid + T * q;
+        group_base<K, C, S::B, S::V>(gi, w);
+        const uint32_t i0 = (uint32_t)base_off + gi % C + (w << p.lb);
+        const uint64_t g_step = g_power(p.tabs, 0, 1u << p.lb);
+        uint64_t s = gl::mul(inv_n, g_power(p.tabs, 0, i0));
 #pragma unroll
-      for (int j = 0; j < NV; j++) {
-        coef[q * NV + j] = gl::mul(coef[q * NV + j], s);
-        if (j + 1 < NV) s = gl::mul(s, g_step);
+        for (int j = 0; j < NV; j++) {
+          coef[q * NV + j] = gl::mul(coef[q * NV + j], s);
+          if (j + 1 < NV) s = gl::mul(s, g_step);
+        }
       }
-    }
-
-    for (uint32_t k = 0; k < nb; k++) {
-      __syncthreads(); // previous coset's stores have read the tile and twiddles
-      fill_twiddles<K>(tws_fwd, p.tabs, 0, brev_bits(k, p.log_blowup), tid, T);
-      __syncthreads();
-      uint64_t x[16];
+      for (uint32_t k = 0; k < nb; k++) {
+        __syncthreads();
+        fill_twiddles<K>(tws_fwd, p.tabs, 0, brev_bits(k, p.log_blowup), tid, T);
+        __syncthreads();
+        uint64_t x[16];
 #pragma unroll
-      for (int j = 0; j < 16; j++) x[j] = coef[j];
-      compute_groups<K, C, false, BB, VV>(x, tws_fwd, tid, T);
-      store_groups<K, C, BB, VV>(tile, x, tid, T);
-      __syncthreads();
-      rounds_from<K, C, false, false, 1>(tile, tws_fwd, tid, T);
-      uint64_t *out = p.out + (uint64_t)k * p.coset_stride;
+        for (int j = 0; j < 16; j++) x[j] = coef[j];
+        compute_groups<K, C, false, S::B, S::V>(x, tws_fwd, tid, T);
+        store_groups<K, C, S::B, S::V>(tile, x, tid, T);
+        __syncthreads();
+        top_store(p, tile, c0, col_end, k, base_off, tid, T);
+      }
+    } else {
+      // inverse stages of the window (bottom-up): the short round first, then the
+      // full rounds; the last full round (top 4 bits) stays in registers, scaled
+      if constexpr (R > 0) rounds_from<K, C, true, true, 0, 1>(tile, tws_inv, tid, T);
+      uint32_t w;
+      const uint32_t eb = gbase16<K, C>(tid, K - 4, w);
+      uint64_t coef[16];
+#pragma unroll 1
+      for (int r = 0; r < NF; r++) {
+        const uint32_t B = (uint32_t)(R + 4 * r);
+        uint32_t wr;
+        const uint32_t ebr = gbase16<K, C>(tid, B, wr);
+        uint32_t a[16];
+        slots16(ebr, (uint32_t)C << B, a);
+        uint64_t x[16];
 #pragma unroll
-      for (int j = 0; j < 8; j++) {
-        const uint32_t e = 2 * (tid + T * j);
-        uint32_t g;
-        uint64_t off;
-        tile_elem<K, C>(e, g, off, base_off, p.lb);
-        const uint32_t col = c0 + g;
-        if (col >= col_end) continue;
-        uint64_t v0 = tile[pad16(e)], v1 = tile[pad16(e) + 1];
-        if (p.canon_out) {
-          v0 = gl::canon(v0);
-          v1 = gl::canon(v1);
-        }
-        uint64_t *dst = out + (uint64_t)col * p.stride_out + off;
-        if (p.vec_out) {
-          *reinterpret_cast<ulonglong2 *>(dst) = make_ulonglong2(v0, v1);
+        for (int j = 0; j < 16; j++) x[j] = tile[a[j]];
+        net16<K, true>(x, tws_inv, wr, B);
+        if (r + 1 < NF) {
+#pragma unroll
+          for (int j = 0; j < 16; j++) tile[a[j]] = x[j];
+          __syncthreads();
         } else {
-          dst[0] = v0;
-          dst[1] = v1;
+#pragma unroll
+          for (int j = 0; j < 16; j++) coef[j] = x[j];
         }
+      }
+      // scale n^-1 g^i: element j of this thread's group has natural index i0 + (j << (lb + K - 4))
+      {
+        const uint32_t i0 = (uint32_t)base_off + tid % C + (w << p.lb);
+        const uint64_t g_step = g_power(p.tabs, 0, 1u << (p.lb + K - 4));
+        uint64_t s = gl::mul(inv_n, g_power(p.tabs, 0, i0));
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+          coef[j] = gl::mul(coef[j], s);
+          if (j + 1 < 16) s = gl::mul(s, g_step);
+        }
+      }
+      for (uint32_t k = 0; k < nb; k++) {
+        __syncthreads(); // previous coset's stores have read the tile and twiddles
+        fill_twiddles<K>(tws_fwd, p.tabs, 0, brev_bits(k, p.log_blowup), tid, T);
+        __syncthreads();
+        // forward stages (top-down): the first full round starts from the registers
+#pragma unroll 1
+        for (int r = 0; r < NF; r++) {
+          const uint32_t B = (uint32_t)(K - 4 - 4 * r);
+          uint32_t wr;
+          const uint32_t ebr = gbase16<K, C>(tid, B, wr);
+          uint32_t a[16];
+          slots16(ebr, (uint32_t)C << B, a);
+          uint64_t x[16];
+          if (r == 0) {
+#pragma unroll
+            for (int j = 0; j < 16; j++) x[j] = coef[j];
+          } else {
+#pragma unroll
+            for (int j = 0; j < 16; j++) x[j] = tile[a[j]];
+          }
+          net16<K, false>(x, tws_fwd, wr, B);
+#pragma unroll
+          for (int j = 0; j < 16; j++) tile[a[j]] = x[j];
+          __syncthreads();
+        }
+        if constexpr (R > 0) rounds_from<K, C, false, false, NF>(tile, tws_fwd, tid, T);
+        top_store(p, tile, c0, col_end, k, base_off, tid, T);
       }
     }
     __syncthreads();
@@ -166,5 +237,11 @@ bool build_lde_steps(const Plan &pl, const uint64_t *in, uint64_t *out, uint32_t
 
 bool lde_args_ok(uint32_t log_n, uint32_t num_cols, uint64_t stride_in, uint64_t stride_out, uint64_t coset_stride,
                  uint32_t log_blowup);
+
+// Launches the fused LDE's kernels on `stream`; events (optional): ev[0] is
+// recorded before the first kernel and ev[j + 1] after kernel j.
+cudaError_t lde_fused(const Plan &pl, const uint64_t *in, uint64_t *out, uint32_t log_n, uint32_t num_cols,
+                      uint64_t stride_in, uint64_t stride_out, uint64_t coset_stride, uint32_t log_blowup,
+                      cudaStream_t stream, cudaEvent_t *ev = nullptr, uint32_t n_ev = 0);
 
 } // namespace bc

@@ -422,10 +422,14 @@ __device__ __forceinline__ void pass_body(const PassParams &p, uint32_t bx, uint
         const uint64_t step = 1ull << (B + p.lb);
 #pragma unroll
         for (int j = 0; j < 16; j++) x[j] = __ldcg(src + j * step);
-        if (p.load_scale) {
+        if (p.load_scale) { // c^i for i = off0 + j * step: a running product
+          const uint64_t c_step = coset_power(p.tabs, 0, (uint32_t)step, p.coset_kshift);
+          uint64_t c = coset_power(p.tabs, 0, (uint32_t)off0, p.coset_kshift);
 #pragma unroll
-          for (int j = 0; j < 16; j++)
-            x[j] = gl::mul(x[j], coset_power(p.tabs, 0, (uint32_t)(off0 + j * step), p.coset_kshift));
+          for (int j = 0; j < 16; j++) {
+            x[j] = gl::mul(x[j], c);
+            if (j + 1 < 16) c = gl::mul(c, c_step);
+          }
         }
       } else {
 #pragma unroll
@@ -493,17 +497,20 @@ __device__ __forceinline__ void pass_body(const PassParams &p, uint32_t bx, uint
         if (col < tg.col_end) {
           uint64_t *dst = out + (uint64_t)col * p.stride_out + off0;
           const uint64_t step = 1ull << (B + p.lb);
-          const uint64_t s = p.tabs.inv_pow2[p.log_n];
-#pragma unroll
-          for (int j = 0; j < 16; j++) {
-            uint64_t v = x[j];
-            if (p.store_scale) {
-              const uint32_t i = (uint32_t)(off0 + j * step); // natural index of a bit-reversed->natural output
-              v = gl::mul(v, p.has_coset ? gl::mul(s, coset_power(p.tabs, 1, i, p.coset_kshift)) : s);
+          if (p.store_scale) { // n^-1 c^-i for the natural index i = off0 + j * step: a running product
+            uint64_t s = p.tabs.inv_pow2[p.log_n], s_step = 1;
+            if (p.has_coset) {
+              s = gl::mul(s, coset_power(p.tabs, 1, (uint32_t)off0, p.coset_kshift));
+              s_step = coset_power(p.tabs, 1, (uint32_t)step, p.coset_kshift);
             }
-            if (p.canon_out) v = gl::canon(v);
-            __stcg(dst + j * step, v);
+#pragma unroll
+            for (int j = 0; j < 16; j++) {
+              x[j] = gl::mul(x[j], s);
+              if (j + 1 < 16) s = gl::mul(s, s_step);
+            }
           }
+#pragma unroll
+          for (int j = 0; j < 16; j++) __stcg(dst + j * step, p.canon_out ? gl::canon(x[j]) : x[j]);
         }
         __syncthreads();
         continue;

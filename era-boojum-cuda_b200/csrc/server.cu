@@ -1,0 +1,367 @@
+// server.cu -- continuous-batching LDE server.
+//
+// No counterpart in the reference (a library of stream-ordered calls).  A
+// server owns, on one device: the twiddle tables (the context), a device
+// arena of `memory_budget_bytes` allocated once at start-up, and `slots`
+// pipelines (three streams each, host_lde.cuh).  Requests carry host buffers
+// (pinned for overlap) and are queued by bc_lde_server_submit; a worker
+// thread admits them in arrival order whenever a slot is free and the arena
+// has room for the request's workspace, so requests that arrive while others
+// are on the GPU join as soon as a slot and memory free up and their copies
+// and kernels overlap on the device.  A request larger than its share of the
+// arena is streamed through in column chunks that fit.  Completion is stamped
+// by a host callback on the request's stream; latency = completion - submit.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstdint>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <new>
+#include <thread>
+#include <vector>
+
+#include "../../include/bc_ntt.h"
+#include "host_lde.cuh"
+
+namespace bc {
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+enum ReqState : int { PENDING = 0, RUNNING = 1, DONE = 2, CANCELLED = 3, FAILED = 4 };
+
+struct Request {
+  uint64_t id;
+  const uint64_t *in;
+  uint64_t *out;
+  uint32_t log_n, cols, log_blowup;
+  Clock::time_point submit, start, finish;
+  int state = PENDING;
+  cudaError_t error = cudaSuccess;
+  // while running
+  int slot = -1;
+  size_t arena_off = 0, arena_bytes = 0;
+};
+
+// First-fit allocator over the device arena (offsets, 256-byte granules).
+struct Arena {
+  size_t size = 0;
+  std::map<size_t, size_t> free_; // offset -> length
+  void init(size_t s) {
+    size = s;
+    free_.clear();
+    free_[0] = s;
+  }
+  bool alloc(size_t bytes, size_t &off) {
+    bytes = (bytes + 255) & ~(size_t)255;
+    for (auto it = free_.begin(); it != free_.end(); ++it) {
+      if (it->second >= bytes) {
+        off = it->first;
+        const size_t rest = it->second - bytes;
+        free_.erase(it);
+        if (rest) free_[off + bytes] = rest;
+        return true;
+      }
+    }
+    return false;
+  }
+  void release(size_t off, size_t bytes) {
+    bytes = (bytes + 255) & ~(size_t)255;
+    auto it = free_.emplace(off, bytes).first;
+    auto nx = std::next(it);
+    if (nx != free_.end() && it->first + it->second == nx->first) {
+      it->second += nx->second;
+      free_.erase(nx);
+    }
+    if (it != free_.begin()) {
+      auto pv = std::prev(it);
+      if (pv->first + pv->second == it->first) {
+        pv->second += it->second;
+        free_.erase(it);
+      }
+    }
+  }
+  size_t largest_free() const {
+    size_t m = 0;
+    for (auto &kv : free_) m = std::max(m, kv.second);
+    return m;
+  }
+};
+
+} // namespace
+} // namespace bc
+
+using namespace bc;
+
+struct bc_lde_server {
+  int device = 0;
+  bc_lde_server_config cfg{};
+  uint64_t *arena_base = nullptr;
+  Arena arena;
+  std::vector<HostPipe> pipes;
+  std::vector<int> slot_busy;
+  std::mutex mu;
+  std::condition_variable cv;      // worker wake-up
+  std::condition_variable done_cv; // request completions
+  std::deque<Request *> pending;
+  std::map<uint64_t, Request *> all;
+  uint64_t next_id = 1;
+  bool stop = false;
+  std::thread worker;
+  // stats
+  uint64_t completed = 0, out_elems = 0;
+  double busy_ms = 0;
+  Clock::time_point first_submit{}, last_finish{};
+  std::vector<double> latencies_ms;
+};
+
+namespace {
+
+struct DoneCtx {
+  bc_lde_server *srv;
+  Request *req;
+};
+
+// Runs on a CUDA driver thread when the request's stream reaches its end;
+// makes no CUDA calls.
+void CUDART_CB on_request_done(void *p) {
+  DoneCtx *d = static_cast<DoneCtx *>(p);
+  {
+    std::lock_guard<std::mutex> lock(d->srv->mu);
+    d->req->finish = Clock::now();
+    d->req->state = DONE;
+  }
+  d->srv->cv.notify_all();
+  d->srv->done_cv.notify_all();
+  delete d;
+}
+
+size_t request_workspace(const bc_lde_server *s, const Request &r, uint32_t &chunk) {
+  const uint64_t per_col = 8ull * ((1ull << r.log_n) + ((1ull << r.log_n) << r.log_blowup));
+  const size_t share = s->cfg.memory_budget_bytes / std::max<uint32_t>(1, s->cfg.slots);
+  uint64_t cols = std::min<uint64_t>(r.cols, share / (per_col * HOST_NBUF));
+  if (s->cfg.max_chunk_cols) cols = std::min<uint64_t>(cols, s->cfg.max_chunk_cols);
+  chunk = (uint32_t)cols;
+  return (size_t)cols * per_col * HOST_NBUF;
+}
+
+// Tries to start the oldest pending request; returns true if one started.
+bool admit_one(bc_lde_server *s, std::unique_lock<std::mutex> &lock) {
+  if (s->pending.empty()) return false;
+  Request *r = s->pending.front();
+  int slot = -1;
+  for (size_t i = 0; i < s->slot_busy.size(); i++)
+    if (!s->slot_busy[i]) {
+      slot = (int)i;
+      break;
+    }
+  if (slot < 0) return false;
+  uint32_t chunk = 0;
+  const size_t bytes = request_workspace(s, *r, chunk);
+  size_t off = 0;
+  if (chunk == 0 || !s->arena.alloc(bytes, off)) return false; // wait for memory to free up
+  s->pending.pop_front();
+  s->slot_busy[slot] = 1;
+  r->slot = slot;
+  r->arena_off = off;
+  r->arena_bytes = bytes;
+  r->state = RUNNING;
+  r->start = Clock::now();
+  lock.unlock(); // enqueue without holding the lock (the done callback takes it)
+  HostPipe &hp = s->pipes[slot];
+  const uint64_t n = 1ull << r->log_n;
+  cudaError_t e = host_lde_enqueue(hp, r->in, r->out, r->log_n, r->cols, n, n, (uint64_t)r->cols * n, r->log_blowup,
+                                   s->arena_base + off / 8, chunk, false, nullptr);
+  if (e == cudaSuccess) e = cudaLaunchHostFunc(hp.s_out, on_request_done, new DoneCtx{s, r});
+  lock.lock();
+  if (e != cudaSuccess) {
+    r->error = e;
+    r->state = FAILED;
+    r->finish = Clock::now();
+    s->done_cv.notify_all();
+  }
+  return true;
+}
+
+void worker_main(bc_lde_server *s) {
+  cudaSetDevice(s->device);
+  std::unique_lock<std::mutex> lock(s->mu);
+  while (!s->stop) {
+    // retire finished requests: free their slot and memory
+    for (auto &kv : s->all) {
+      Request *r = kv.second;
+      if ((r->state == DONE || r->state == FAILED) && r->slot >= 0) {
+        s->slot_busy[r->slot] = 0;
+        s->arena.release(r->arena_off, r->arena_bytes);
+        r->slot = -1;
+        if (r->state == DONE) {
+          const double lat = std::chrono::duration<double, std::milli>(r->finish - r->submit).count();
+          s->latencies_ms.push_back(lat);
+          s->completed++;
+          s->out_elems += ((uint64_t)r->cols << r->log_n) << r->log_blowup;
+          if (r->finish > s->last_finish) s->last_finish = r->finish;
+        }
+      }
+    }
+    while (admit_one(s, lock)) {
+    }
+    s->cv.wait_for(lock, std::chrono::milliseconds(5));
+  }
+}
+
+} // namespace
+
+extern "C" cudaError_t bc_lde_server_create(const bc_lde_server_config *cfg, bc_lde_server **out) {
+  if (!cfg || !out || cfg->slots == 0 || cfg->slots > 64 || cfg->memory_budget_bytes < (1u << 20))
+    return cudaErrorInvalidValue;
+  *out = nullptr;
+  cudaError_t e = bc_ntt_context_create(12, 12);
+  if (e != cudaSuccess) return e;
+  bc_lde_server *s = new (std::nothrow) bc_lde_server();
+  if (!s) return cudaErrorMemoryAllocation;
+  s->cfg = *cfg;
+  cudaGetDevice(&s->device);
+  e = cudaMalloc(&s->arena_base, cfg->memory_budget_bytes);
+  if (e != cudaSuccess) {
+    delete s;
+    return e;
+  }
+  s->arena.init(cfg->memory_budget_bytes);
+  s->pipes.resize(cfg->slots);
+  s->slot_busy.assign(cfg->slots, 0);
+  for (auto &p : s->pipes) {
+    if ((e = host_pipe_init(p)) != cudaSuccess) {
+      for (auto &q : s->pipes) host_pipe_destroy(q);
+      cudaFree(s->arena_base);
+      delete s;
+      return e;
+    }
+  }
+  s->worker = std::thread(worker_main, s);
+  *out = s;
+  return cudaSuccess;
+}
+
+extern "C" cudaError_t bc_lde_server_submit(bc_lde_server *s, const uint64_t *host_evals_bitrev, uint64_t *host_out,
+                                            uint32_t log_n, uint32_t num_cols, uint32_t log_blowup,
+                                            uint64_t *request_id) {
+  if (!s || !host_evals_bitrev || !host_out || !request_id || num_cols == 0) return cudaErrorInvalidValue;
+  const uint64_t n = 1ull << log_n;
+  if (!lde_args_ok(log_n, num_cols, n, n, (uint64_t)num_cols * n, log_blowup)) return cudaErrorInvalidValue;
+  // a request must fit the arena at least one column at a time
+  const uint64_t per_col = 8ull * (n + (n << log_blowup));
+  if (per_col * HOST_NBUF > s->cfg.memory_budget_bytes / s->cfg.slots) return cudaErrorInvalidValue;
+  Request *r = new (std::nothrow) Request();
+  if (!r) return cudaErrorMemoryAllocation;
+  r->in = host_evals_bitrev;
+  r->out = host_out;
+  r->log_n = log_n;
+  r->cols = num_cols;
+  r->log_blowup = log_blowup;
+  r->submit = Clock::now();
+  {
+    std::lock_guard<std::mutex> lock(s->mu);
+    r->id = s->next_id++;
+    if (s->first_submit == Clock::time_point{}) s->first_submit = r->submit;
+    s->all[r->id] = r;
+    s->pending.push_back(r);
+    *request_id = r->id;
+  }
+  s->cv.notify_all();
+  return cudaSuccess;
+}
+
+// state: 0 pending, 1 running, 2 done, 3 cancelled, 4 failed (see *error).
+extern "C" cudaError_t bc_lde_server_poll(bc_lde_server *s, uint64_t id, int *state, double *latency_ms) {
+  if (!s || !state) return cudaErrorInvalidValue;
+  std::lock_guard<std::mutex> lock(s->mu);
+  auto it = s->all.find(id);
+  if (it == s->all.end()) return cudaErrorInvalidValue;
+  Request *r = it->second;
+  *state = r->state;
+  if (latency_ms)
+    *latency_ms = (r->state == DONE) ? std::chrono::duration<double, std::milli>(r->finish - r->submit).count() : -1.0;
+  return r->state == FAILED ? r->error : cudaSuccess;
+}
+
+extern "C" cudaError_t bc_lde_server_wait(bc_lde_server *s, uint64_t id, uint32_t timeout_ms, double *latency_ms) {
+  if (!s) return cudaErrorInvalidValue;
+  std::unique_lock<std::mutex> lock(s->mu);
+  auto it = s->all.find(id);
+  if (it == s->all.end()) return cudaErrorInvalidValue;
+  Request *r = it->second;
+  const bool ok = s->done_cv.wait_for(lock, std::chrono::milliseconds(timeout_ms),
+                                      [&] { return r->state == DONE || r->state == FAILED || r->state == CANCELLED; });
+  if (!ok) return cudaErrorTimeout;
+  if (latency_ms)
+    *latency_ms = (r->state == DONE) ? std::chrono::duration<double, std::milli>(r->finish - r->submit).count() : -1.0;
+  if (r->state == FAILED) return r->error;
+  if (r->state == CANCELLED) return cudaErrorNotReady;
+  return cudaSuccess;
+}
+
+// Cancels a request that has not been admitted yet (cudaErrorNotReady if it already runs or ran).
+extern "C" cudaError_t bc_lde_server_cancel(bc_lde_server *s, uint64_t id) {
+  if (!s) return cudaErrorInvalidValue;
+  std::lock_guard<std::mutex> lock(s->mu);
+  auto it = s->all.find(id);
+  if (it == s->all.end()) return cudaErrorInvalidValue;
+  Request *r = it->second;
+  if (r->state != PENDING) return cudaErrorNotReady;
+  s->pending.erase(std::remove(s->pending.begin(), s->pending.end(), r), s->pending.end());
+  r->state = CANCELLED;
+  s->done_cv.notify_all();
+  return cudaSuccess;
+}
+
+extern "C" cudaError_t bc_lde_server_get_stats(bc_lde_server *s, bc_lde_server_stats *st) {
+  if (!s || !st) return cudaErrorInvalidValue;
+  std::lock_guard<std::mutex> lock(s->mu);
+  *st = bc_lde_server_stats{};
+  st->completed = s->completed;
+  uint64_t pend = 0, run = 0;
+  for (auto &kv : s->all) {
+    pend += kv.second->state == PENDING;
+    run += kv.second->state == RUNNING;
+  }
+  st->pending = pend;
+  st->running = run;
+  std::vector<double> l = s->latencies_ms;
+  std::sort(l.begin(), l.end());
+  auto pct = [&](double q) { return l.empty() ? 0.0 : l[std::min(l.size() - 1, (size_t)(q * (l.size() - 1) + 0.5))]; };
+  st->p50_ms = pct(0.50);
+  st->p99_ms = pct(0.99);
+  st->max_ms = l.empty() ? 0.0 : l.back();
+  const double span = std::chrono::duration<double>(s->last_finish - s->first_submit).count();
+  st->span_s = span > 0 ? span : 0;
+  st->out_melem_per_s = span > 0 ? (double)s->out_elems / span / 1e6 : 0;
+  st->arena_largest_free = s->arena.largest_free();
+  return cudaSuccess;
+}
+
+extern "C" cudaError_t bc_lde_server_destroy(bc_lde_server *s) {
+  if (!s) return cudaErrorInvalidValue;
+  {
+    std::lock_guard<std::mutex> lock(s->mu);
+    s->stop = true;
+    for (Request *r : s->pending) r->state = CANCELLED;
+    s->pending.clear();
+  }
+  s->cv.notify_all();
+  s->worker.join();
+  cudaError_t e = cudaSuccess;
+  for (auto &p : s->pipes) {
+    cudaError_t e2 = cudaStreamSynchronize(p.s_out);
+    if (e2 != cudaSuccess) e = e2;
+  }
+  cudaDeviceSynchronize(); // host callbacks of finished requests have run
+  for (auto &p : s->pipes) host_pipe_destroy(p);
+  cudaFree(s->arena_base);
+  for (auto &kv : s->all) delete kv.second;
+  delete s;
+  return e;
+}

@@ -116,6 +116,22 @@ cudaError_t bc_lde_fused_profiled(const uint64_t *evals_bitrev, uint64_t *out, u
                                   uint32_t log_blowup, cudaStream_t stream, cudaEvent_t *events, uint32_t num_events,
                                   uint32_t *num_kernels);
 
+/* Coset LDE from HOST memory to HOST memory (same layouts and meaning as
+ * bc_lde_fused, host pointers).  No counterpart in the reference, whose
+ * callers copy in, transform and copy out one step after the other.  Columns
+ * are processed in chunks cycling through three device buffers carved from
+ * the caller's `workspace` (device memory, workspace_bytes long; nothing is
+ * allocated), so copy-in, transform and copy-out of consecutive chunks
+ * overlap.  A chunk holds min(max_chunk_cols (0 = no limit), what fits)
+ * columns; the workspace must hold at least 3 x 8 x n x (1 + 2^log_blowup)
+ * bytes.  Host buffers should be pinned for the overlap.  Asynchronous:
+ * `stream` waits for the whole operation; the host output is complete once
+ * the stream has reached this point.  Calls sharing a workspace must not be
+ * in flight at the same time. */
+cudaError_t bc_lde_host(const uint64_t *host_evals_bitrev, uint64_t *host_out, uint32_t log_n, uint32_t num_cols,
+                        uint64_t stride_in, uint64_t stride_out, uint64_t coset_stride, uint32_t log_blowup,
+                        uint64_t *workspace, size_t workspace_bytes, uint32_t max_chunk_cols, cudaStream_t stream);
+
 /* ---- uneven batches of LDE jobs in one persistent launch ------------------
  * No counterpart in the reference, whose callers issue 1 + B batch_ntt calls
  * per job (src/ntt.rs:179-191), each of 2-3 kernels, or log_n kernels for
@@ -162,6 +178,45 @@ cudaError_t bc_lde_batch_plan_destroy(bc_lde_batch_plan *plan);
  * the batch status word (bit 0: a bounded dependency wait expired and the
  * outputs are invalid). */
 cudaError_t bc_lde_batch_noalloc(const bc_lde_job *jobs, uint32_t n_jobs, cudaStream_t stream, uint32_t *status);
+
+/* ---- continuous-batching LDE server ---------------------------------------
+ * No counterpart in the reference.  One server per device: it creates the
+ * context, allocates a device arena of memory_budget_bytes ONCE, and runs
+ * `slots` pipelines.  Requests (host buffers, pinned for overlap; dense
+ * layouts: column j at j * n, coset k of column j at (k * num_cols + j) * n)
+ * are admitted in arrival order whenever a slot is free and the arena has
+ * room for their workspace -- requests arriving while others run join as
+ * slots and memory free up, and their copies and kernels overlap on the GPU.
+ * A request bigger than its arena share (budget / slots) is streamed through
+ * in column chunks.  Submit never blocks on the GPU. */
+typedef struct bc_lde_server_config {
+  size_t memory_budget_bytes; /* device memory the server holds for requests */
+  uint32_t slots;             /* requests on the GPU at once (1..64) */
+  uint32_t max_chunk_cols;    /* 0: chunks as large as a slot's share allows */
+} bc_lde_server_config;
+
+typedef struct bc_lde_server_stats {
+  uint64_t completed, pending, running;
+  double p50_ms, p99_ms, max_ms; /* latency = completion - submit, completed requests */
+  double span_s;                 /* first submit to last completion */
+  double out_melem_per_s;        /* output elements of completed requests / span */
+  size_t arena_largest_free;
+} bc_lde_server_stats;
+
+typedef struct bc_lde_server bc_lde_server;
+
+cudaError_t bc_lde_server_create(const bc_lde_server_config *cfg, bc_lde_server **server);
+cudaError_t bc_lde_server_submit(bc_lde_server *server, const uint64_t *host_evals_bitrev, uint64_t *host_out,
+                                 uint32_t log_n, uint32_t num_cols, uint32_t log_blowup, uint64_t *request_id);
+/* *state: 0 pending, 1 running, 2 done, 3 cancelled, 4 failed (the call returns the error). */
+cudaError_t bc_lde_server_poll(bc_lde_server *server, uint64_t request_id, int *state, double *latency_ms);
+/* Waits up to timeout_ms: cudaErrorTimeout if still unfinished, cudaErrorNotReady if cancelled. */
+cudaError_t bc_lde_server_wait(bc_lde_server *server, uint64_t request_id, uint32_t timeout_ms, double *latency_ms);
+/* Cancels a request not yet admitted (cudaErrorNotReady once it runs or ran). */
+cudaError_t bc_lde_server_cancel(bc_lde_server *server, uint64_t request_id);
+cudaError_t bc_lde_server_get_stats(bc_lde_server *server, bc_lde_server_stats *stats);
+/* Cancels pending requests, waits for running ones, frees everything. */
+cudaError_t bc_lde_server_destroy(bc_lde_server *server);
 
 #ifdef __cplusplus
 }
