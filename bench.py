@@ -46,6 +46,20 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
+def measured_traffic(log_n: int, log_blowup: int, cols: int):
+    """DRAM bytes of one top-window launch from the committed ncu summary, scaled to `cols` columns."""
+    path = os.path.join(ROOT, "profiles", f"lde_top_kernel_traffic_logn{log_n}_blowup{1 << log_blowup}.txt")
+    try:
+        for line in open(path):
+            if line.startswith("kernel="):
+                kv = dict(tok.split("=", 1) for tok in line.split())
+                if int(kv["log_n"]) == log_n and int(kv["log_blowup"]) == log_blowup:
+                    return round((int(kv["dram_read"]) + int(kv["dram_write"])) * cols / int(kv["cols"]))
+    except OSError:
+        pass
+    return None
+
+
 class ClockSampler:
     """SM clock / throttle-reason samples during the timed region, read in-process through NVML.
 
@@ -274,13 +288,16 @@ def run_ours(args, rank, world):
                    (1 + B) * col_bytes)]
                + [(f"lde forward pass {i} (n2b, all cosets)", 2 * B * col_bytes) for i in range(npass - 1)])
     roofline = None
+    traffic = measured_traffic(LOG_N, LOG_BLOWUP, COLS)
     if kern_ms and len(kern_ms) == len(kernels):
         dom = max(range(len(kern_ms)), key=lambda i: kern_ms[i])
         name, byts = kernels[dom]
         achieved = byts / (kern_ms[dom] / 1e3) / 1e9
         roofline = {"bound": "hbm", "kernel": name, "achieved": round(achieved, 1), "peak": peak,
                     "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
-                    "traffic": None, "kernel_ms": [round(v, 3) for v in kern_ms],
+                    "traffic": traffic if "lde_top_kernel" in name else None,
+                    "traffic_unit": "bytes per launch (ncu dram read+write, scaled from the profiled case)",
+                    "kernel_ms": [round(v, 3) for v in kern_ms],
                     "step_algorithmic_frac": round(8 * n * COLS * (1 + B) / (ms_per_step / 1e3) / 1e9 / peak, 4)}
 
     # end to end through the C ABI with host buffers: bc_lde_host takes pinned host input and writes pinned
@@ -393,7 +410,12 @@ def run_batch_section(reps: int = 3):
 
 
 def run_serve_section(n_requests: int = 48, rate: float = 20.0, budget_gib: int = 40, slots: int = 4):
-    """Poisson LDE requests through the continuous-batching server vs the same requests served one at a time."""
+    """Poisson LDE requests through the continuous-batching server vs the same requests served one at a time.
+
+    latency: requests arrive at `rate`/s; p50/p99 of completion - arrival, beside the FCFS one-at-a-time
+             plain path fed the same arrivals (its queueing computed from measured per-request service times).
+    capacity: all requests queued at once; output Melem/s of the server vs the one-at-a-time plain path.
+    """
     import torch
 
     import bc_ntt
@@ -402,43 +424,65 @@ def run_serve_section(n_requests: int = 48, rate: float = 20.0, budget_gib: int 
     reqs = workloads.serving_stream(n_requests=n_requests, rate_per_s=rate, seed=7)
     max_in = max(r.in_words for r in reqs)
     max_out = max(r.out_words for r in reqs)
+    out_elems = sum(r.out_words for r in reqs)
     # host pools reused by every request (timing; per-request exactness is covered by tests/test_server_gpu.py)
     hin = torch.randint(0, 2**62, (max_in,), dtype=torch.int64).pin_memory()
     hout = torch.empty(max_out, dtype=torch.int64).pin_memory()
-    srv = bc_ntt.LdeServer(memory_budget_bytes=budget_gib << 30, slots=slots)
-    t0 = time.perf_counter()
-    ids = []
-    for r in reqs:
-        d = t0 + r.arrival_s - time.perf_counter()
-        if d > 0:
-            time.sleep(d)
-        ids.append(srv.submit(hin, hout, r.log_n, r.cols, r.log_blowup))
-    for i in ids:
-        srv.wait(i, timeout_ms=600000)
-    wall = time.perf_counter() - t0
-    st = srv.stats()
-    srv.close()
-    # the same requests, one at a time through the plain path (copy in, bc_lde_plain, copy out)
+
+    # one at a time through the plain path: copy in, bc_lde_plain, copy out; service time of each request
     dev_in = torch.empty(max_in, dtype=torch.int64, device="cuda")
     dev_out = torch.empty(max_out, dtype=torch.int64, device="cuda")
+    stream = torch.cuda.current_stream()
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(len(reqs) + 1)]
     torch.cuda.synchronize()
-    t1 = time.perf_counter()
-    for r in reqs:
+    evs[0].record(stream)
+    for i, r in enumerate(reqs):
         dev_in[:r.in_words].copy_(hin[:r.in_words], non_blocking=True)
         bc_ntt.lde(dev_in, dev_out, r.log_n, r.cols, r.log_blowup, fused=False)
         hout[:r.out_words].copy_(dev_out[:r.out_words], non_blocking=True)
+        evs[i + 1].record(stream)
     torch.cuda.synchronize()
-    serial = time.perf_counter() - t1
-    out_elems = sum(r.out_words for r in reqs)
-    del dev_in, dev_out, hin, hout
+    service = [evs[i].elapsed_time(evs[i + 1]) for i in range(len(reqs))]
+    serial_s = sum(service) / 1e3
+    del dev_in, dev_out
     torch.cuda.empty_cache()
-    return {"workload": f"{n_requests} Poisson requests at {rate}/s, log_n U{{14..22}}, cols log-U[8,512], "
-                        f"blowup U{{2,4}}, seed 7, host buffers (pinned)",
-            "budget_gib": budget_gib, "slots": slots, "p50_ms": round(st["p50_ms"], 2), "p99_ms": round(st["p99_ms"], 2),
-            "max_ms": round(st["max_ms"], 2), "value": round(st["out_melem_per_s"], 1),
-            "wall_s": round(wall, 3), "serial_plain_s": round(serial, 3),
-            "serial_plain_value": round(out_elems / serial / 1e6, 1), "unit": "Melem/s",
-            "completed": st["completed"]}
+    # FCFS single-server latencies of the plain path under the same arrivals
+    t_free, lat_serial = 0.0, []
+    for r, sv in zip(reqs, service):
+        start = max(r.arrival_s * 1e3, t_free)
+        t_free = start + sv
+        lat_serial.append(t_free - r.arrival_s * 1e3)
+
+    def serve(arrivals):
+        srv = bc_ntt.LdeServer(memory_budget_bytes=budget_gib << 30, slots=slots)
+        t0 = time.perf_counter()
+        ids = []
+        for r, at in zip(reqs, arrivals):
+            d = t0 + at - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            ids.append(srv.submit(hin, hout, r.log_n, r.cols, r.log_blowup))
+        for i in ids:
+            srv.wait(i, timeout_ms=600000)
+        st = srv.stats()
+        srv.close()
+        return st
+
+    st_lat = serve([r.arrival_s for r in reqs])
+    st_cap = serve([0.0] * len(reqs))
+    del hin, hout
+    return {"workload": f"{n_requests} requests, log_n U{{14..22}}, cols log-U[8,512], blowup U{{2,4}}, seed 7, "
+                        f"pinned host buffers, {budget_gib} GiB budget, {slots} slots",
+            "unit": "Melem/s",
+            "latency": {"rate_per_s": rate, "p50_ms": round(st_lat["p50_ms"], 2), "p99_ms": round(st_lat["p99_ms"], 2),
+                        "max_ms": round(st_lat["max_ms"], 2),
+                        "serial_plain_same_arrivals_p50_ms": round(pct(lat_serial, 50), 2),
+                        "serial_plain_same_arrivals_p99_ms": round(pct(lat_serial, 99), 2)},
+            "capacity": {"server_value": round(st_cap["out_melem_per_s"], 1),
+                         "serial_plain_value": round(out_elems / serial_s / 1e6, 1),
+                         "speedup": round(st_cap["out_melem_per_s"] / (out_elems / serial_s / 1e6), 3),
+                         "server_span_s": round(st_cap["span_s"], 3), "serial_plain_s": round(serial_s, 3)},
+            "completed": int(st_lat["completed"] + st_cap["completed"])}
 
 
 def run_reference(args, rank, world):
