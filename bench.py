@@ -226,6 +226,7 @@ def run_ours(args, rank, world):
     B = 1 << LOG_BLOWUP
     L = bc_ntt.lib()
     bc_ntt.Context.create(12, 12)
+    tuned = bc_ntt.load_tuned_plans() if not args.no_tuned_plans else False
     stream = torch.cuda.current_stream()
     s_handle = stream.cuda_stream
     x = make_inputs(1234 + rank)
@@ -327,6 +328,7 @@ def run_ours(args, rank, world):
         "vs_baseline": None, "dtype": "u64 (Goldilocks)", "data": "synthetic",
         "config": {"workload": f"coset LDE {COLS} cols x 2^{LOG_N}, blowup {B}, bit-reversed in/out",
                    "log_n": LOG_N, "columns": COLS, "blowup": B, "path": "bc_lde_fused",
+                   "plans": "autotuned (era-boojum-cuda_b200/plans_b200.txt)" if tuned else "built-in",
                    "l2": "inputs 4 GiB and outputs 8 GiB, larger than L2; no flush", "parallelism": f"replicas x{world}"},
         "p50_ms": round(pct(per, 50), 4), "p99_ms": round(pct(per, 99), 4),
         "plain": {"value": round(world * len(plain_per) * out_elems / (plain_ms / 1e3) / 1e6, 1),
@@ -346,6 +348,9 @@ def run_ours(args, rank, world):
     torch.cuda.empty_cache()
     if world == 1 and not args.no_batch:
         line["batch"] = run_batch_section()
+        line["batch_small_jobs"] = run_small_batch_section()
+    if world == 1 and not args.no_large:
+        line["large"] = run_large_section()
     if world == 1 and not args.no_serve:
         line["serve"] = run_serve_section()
     return line
@@ -407,6 +412,88 @@ def run_batch_section(reps: int = 3):
             "per_job_plain": {"ms": round(t_plain, 2), "value": mel(t_plain)},
             "persistent_vs_plain": round(t_plain / t_batch, 3), "fused_vs_plain": round(t_plain / t_fused, 3),
             "bit_exact_persistent_vs_per_job": bool(exact), "unit": "Melem/s"}
+
+
+def run_small_batch_section(reps: int = 5):
+    """Many small uneven jobs (log_n 10..16, 1..8 columns): where one launch per job is launch-bound."""
+    import torch
+
+    import bc_ntt
+    import workloads
+
+    specs = workloads.uneven_batch(n_jobs=256, seed=11, log_n_range=(10, 16), cols_range=(1, 8))
+    tens = _uneven_tensors(specs)
+    plan = bc_ntt.LdeBatch(tens)
+    stream = torch.cuda.current_stream()
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    out_elems = sum(sp.out_words for sp in specs)
+    t_batch = timed(plan.run)
+    status = plan.status()
+    first = [t[1].clone() for t in tens]
+    t_fused = timed(lambda: [bc_ntt.lde(*t, fused=True) for t in tens])
+    exact = all(torch.equal(a, t[1]) for a, t in zip(first, tens))
+    t_plain = timed(lambda: [bc_ntt.lde(*t, fused=False) for t in tens])
+    plan.close()
+    del tens, first
+    torch.cuda.empty_cache()
+    mel = lambda ms: round(out_elems / (ms / 1e3) / 1e6, 1)  # noqa: E731
+    return {"workload": "256 jobs, log_n U{10..16}, cols log-U[1,8], blowup U{2,4,8}, seed 11",
+            "persistent_one_launch": {"ms": round(t_batch, 3), "value": mel(t_batch), "status": status},
+            "per_job_fused": {"ms": round(t_fused, 3), "value": mel(t_fused)},
+            "per_job_plain": {"ms": round(t_plain, 3), "value": mel(t_plain)},
+            "persistent_vs_plain": round(t_plain / t_batch, 2), "persistent_vs_fused": round(t_fused / t_batch, 2),
+            "bit_exact_persistent_vs_per_job": bool(exact), "unit": "Melem/s"}
+
+
+def run_large_section(reps: int = 5):
+    """64 columns x 2^23 at blowup 4 (16 GiB out): fused vs the unfused plain composition."""
+    import torch
+
+    import bc_ntt
+
+    log_n, cols, log_b = 23, 64, 2
+    n, B = 1 << log_n, 1 << log_b
+    g = torch.Generator(device="cuda").manual_seed(77)
+    x = torch.randint(-(2**63), 2**63 - 1, (cols * n,), device="cuda", dtype=torch.int64, generator=g)
+    x = torch.where((x < 0) & (x >= -(2**32 - 1)), x + (2**32 - 1), x)
+    out = torch.empty(B * cols * n, dtype=torch.int64, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def timed(fused):
+        bc_ntt.lde(x, out, log_n, cols, log_b, fused=fused)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            bc_ntt.lde(x, out, log_n, cols, log_b, fused=fused)
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    t_f = timed(True)
+    ref = out.clone()
+    t_p = timed(False)
+    exact = bool(torch.equal(ref, out))
+    del x, out, ref
+    torch.cuda.empty_cache()
+    peak, _ = measured_peaks()
+    alg = 8 * n * cols * (1 + B)
+    return {"workload": "coset LDE 64 cols x 2^23, blowup 4 (16 GiB out)",
+            "fused_ms": round(t_f, 3), "plain_ms": round(t_p, 3), "fused_vs_plain": round(t_p / t_f, 3),
+            "fused_value": round(B * n * cols / (t_f / 1e3) / 1e6, 1), "unit": "Melem/s",
+            "fused_hbm_frac": round(alg / (t_f / 1e3) / 1e9 / peak, 4),
+            "plain_hbm_frac": round(alg / (t_p / 1e3) / 1e9 / peak, 4), "bit_exact_fused_vs_plain": exact}
 
 
 def run_serve_section(n_requests: int = 48, rate: float = 20.0, budget_gib: int = 40, slots: int = 4):
@@ -550,6 +637,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the uneven-batch section")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving section")
+    ap.add_argument("--no-large", action="store_true", help="skip the 64 x 2^23 blowup-4 section")
+    ap.add_argument("--no-tuned-plans", action="store_true", help="ignore the autotuned plan file")
     ap.add_argument("--log-n", type=int, default=22, help="column length 2^log_n (default 22)")
     ap.add_argument("--cols", type=int, default=128, help="columns (default 128)")
     ap.add_argument("--log-blowup", type=int, default=1, help="log2 of the blowup (default 1)")

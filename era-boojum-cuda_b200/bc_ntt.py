@@ -48,6 +48,10 @@ SIGNATURES = {
     "bc_batch_ntt_out_of_place": [_vp, _sz, _vp, _sz, _u32, _u32, _u64, _u64, _u64, _u64, _b, _b, _u32, _u32, _vp],
     "bc_batch_ntt_in_place": [_vp, _sz, _u32, _u32, _u64, _u64, _b, _b, _u32, _u32, _vp],
     "bc_batch_ntt_with_plan": [_vp, _vp, _u32, _u32, _u64, _u64, _b, _b, _u32, _u32, _vp, _vp, _u32, _vp],
+    "bc_autotune": [_u32, _u32, _u32, _u32, _vp, _sz],
+    "bc_plan_table_export": [_vp, _sz, _vp],
+    "bc_plan_table_import": [ctypes.c_char_p],
+    "bc_plan_table_clear": [],
     "bc_lde_plain": [_vp, _vp, _u32, _u32, _u64, _u64, _u64, _u32, _vp],
     "bc_lde_fused": [_vp, _vp, _u32, _u32, _u64, _u64, _u64, _u32, _vp],
     "bc_lde_fused_profiled": [_vp, _vp, _u32, _u32, _u64, _u64, _u64, _u32, _vp, _vp, _u32, _vp],
@@ -305,3 +309,38 @@ class LdeServer:
             _check(lib().bc_lde_server_destroy(self.handle), "bc_lde_server_destroy")
             self.handle = ctypes.c_void_p()
             self._keep.clear()
+
+
+def autotune(log_n: int, log_blowup: int, num_cols: int, reps: int = 3) -> str:
+    """Times every candidate plan for (log_n, log_blowup) on the current device and keeps the fastest."""
+    buf = ctypes.create_string_buffer(8192)
+    _check(lib().bc_autotune(log_n, log_blowup, num_cols, reps, buf, len(buf)), "bc_autotune")
+    return buf.value.decode()
+
+
+def plan_table_export() -> str:
+    need = ctypes.c_size_t(0)
+    _check(lib().bc_plan_table_export(None, 0, ctypes.byref(need)), "bc_plan_table_export")
+    buf = ctypes.create_string_buffer(max(1, need.value))
+    _check(lib().bc_plan_table_export(buf, len(buf), None), "bc_plan_table_export")
+    return buf.value.decode()
+
+
+def plan_table_import(text: str):
+    _check(lib().bc_plan_table_import(text.encode()), "bc_plan_table_import")
+
+
+def plan_table_clear():
+    _check(lib().bc_plan_table_clear(), "bc_plan_table_clear")
+
+
+PLANS_PATH = os.path.join(_HERE, "plans_b200.txt")
+
+
+def load_tuned_plans(path: str = PLANS_PATH) -> bool:
+    """Loads a plan table written by tune_plans.py (the current device must have a context)."""
+    if not os.path.exists(path):
+        return False
+    text = "".join(line for line in open(path) if line.strip() and not line.startswith("#"))
+    plan_table_import(text)
+    return True

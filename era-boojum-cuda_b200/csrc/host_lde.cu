@@ -68,7 +68,7 @@ cudaError_t host_lde_enqueue(HostPipe &hp, const uint64_t *host_in, uint64_t *ho
                              cudaStream_t caller) {
   const uint64_t n = 1ull << log_n, nb = 1ull << log_blowup;
   const uint64_t in_words = (uint64_t)chunk * n, out_words = in_words * nb;
-  const Plan pl = default_plan(log_n);
+  const Plan pl = tuned_plan(log_n, log_blowup);
   cudaError_t e;
 #define CK(x)                                                                                                          \
   if ((e = (x)) != cudaSuccess) return e;

@@ -261,7 +261,7 @@ extern "C" cudaError_t bc_lde_fused(const uint64_t *evals_bitrev, uint64_t *out,
                                     uint32_t log_blowup, cudaStream_t stream) {
   if (!lde_args_ok(log_n, num_cols, stride_in, stride_out, coset_stride, log_blowup)) return cudaErrorInvalidValue;
   if (num_cols && (!evals_bitrev || !out)) return cudaErrorInvalidValue;
-  return lde_fused(default_plan(log_n), evals_bitrev, out, log_n, num_cols, stride_in, stride_out, coset_stride,
+  return lde_fused(tuned_plan(log_n, log_blowup), evals_bitrev, out, log_n, num_cols, stride_in, stride_out, coset_stride,
                    log_blowup, stream);
 }
 
@@ -271,7 +271,7 @@ extern "C" cudaError_t bc_lde_fused_profiled(const uint64_t *evals_bitrev, uint6
                                              cudaEvent_t *events, uint32_t num_events, uint32_t *num_kernels) {
   if (!lde_args_ok(log_n, num_cols, stride_in, stride_out, coset_stride, log_blowup)) return cudaErrorInvalidValue;
   if (num_cols && (!evals_bitrev || !out)) return cudaErrorInvalidValue;
-  const Plan pl = default_plan(log_n);
+  const Plan pl = tuned_plan(log_n, log_blowup);
   if (num_kernels) *num_kernels = (uint32_t)(2 * pl.npasses - 1);
   return lde_fused(pl, evals_bitrev, out, log_n, num_cols, stride_in, stride_out, coset_stride, log_blowup, stream,
                    events, num_events);

@@ -191,14 +191,19 @@ cudaError_t schedule(const bc_lde_job *jobs, uint32_t n_jobs, std::vector<BatchR
     if (!lde_args_ok(jb.log_n, jb.num_cols, jb.stride_in, jb.stride_out, jb.coset_stride, jb.log_blowup))
       return cudaErrorInvalidValue;
     if (jb.num_cols && (!jb.evals_bitrev || !jb.out)) return cudaErrorInvalidValue;
-    if (!build_lde_steps(default_plan(jb.log_n), jb.evals_bitrev, jb.out, jb.log_n, jb.num_cols, jb.stride_in,
-                         jb.stride_out, jb.coset_stride, jb.log_blowup, true, 4, steps[j]))
+    // the tuned plan, or the built-in one when the tuned plan uses a window shape this kernel does not carry
+    auto build = [&](const Plan &pl) {
+      if (!build_lde_steps(pl, jb.evals_bitrev, jb.out, jb.log_n, jb.num_cols, jb.stride_in, jb.stride_out,
+                           jb.coset_stride, jb.log_blowup, true, 4, steps[j]))
+        return false;
+      for (const LdeStep &st : steps[j])
+        if (!batch_shape_supported(shape_id(st.top, st.b2n, st.K, st.C)) || st.threads != BATCH_THREADS ||
+            st.smem > BATCH_SMEM_BYTES || st.grid.x >= (1u << 28) || st.grid.y >= (1u << 20))
+          return false;
+      return true;
+    };
+    if (!build(tuned_plan(jb.log_n, jb.log_blowup)) && !build(default_plan(jb.log_n)))
       return cudaErrorInvalidConfiguration;
-    for (const LdeStep &st : steps[j]) {
-      if (!batch_shape_supported(shape_id(st.top, st.b2n, st.K, st.C)) || st.threads != BATCH_THREADS ||
-          st.smem > BATCH_SMEM_BYTES || st.grid.x >= (1u << 28) || st.grid.y >= (1u << 20))
-        return cudaErrorInvalidConfiguration;
-    }
     max_depth = std::max(max_depth, steps[j].size());
   }
   // big jobs first within every depth

@@ -407,7 +407,7 @@ extern "C" cudaError_t bc_batch_ntt_internal(const uint64_t *inputs, uint64_t *o
                                              uint32_t coset_index, cudaStream_t stream) {
   if (!ntt_args_ok(log_n, stride_in, stride_out, log_extension_degree, coset_index)) return cudaErrorInvalidValue;
   if (num_ntts && (!inputs || !outputs)) return cudaErrorInvalidValue;
-  return launch_ntt(default_plan(log_n), inputs, outputs, log_n, num_ntts, stride_in, stride_out, bitrev_inputs,
+  return launch_ntt(tuned_plan(log_n, 0), inputs, outputs, log_n, num_ntts, stride_in, stride_out, bitrev_inputs,
                     inverse, log_extension_degree, coset_index, stream);
 }
 

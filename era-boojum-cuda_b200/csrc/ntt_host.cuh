@@ -30,6 +30,9 @@ int current_device();
 int sm_count();
 
 Plan default_plan(uint32_t log_n);
+// The autotuned plan of the current device for an LDE (log_blowup >= 1) or a
+// plain NTT (log_blowup = 0), else default_plan (tune.cu).
+Plan tuned_plan(uint32_t log_n, uint32_t log_blowup);
 bool plan_valid(const Plan &pl, uint32_t log_n);
 
 // One pass over columns that may come in 2^log_groups groups (see ntt_pass.cuh).

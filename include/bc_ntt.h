@@ -79,6 +79,25 @@ cudaError_t bc_batch_ntt_with_plan(const uint64_t *inputs, uint64_t *outputs, ui
                                    uint32_t log_extension_degree, uint32_t coset_index, const uint8_t *pass_bits,
                                    const uint8_t *pass_runs, uint32_t npasses, cudaStream_t stream);
 
+/* ---- plans and the autotuner ------------------------------------------------
+ * Replace the reference's fixed PLANS table (src/ntt.rs:74-169).  A plan says
+ * how log_n index bits split into passes (the radix split), which run of
+ * consecutive positions each pass's tiles span (the tile shape), and -- for
+ * the fused LDE -- how many stages its middle kernel fuses (the top window).
+ * Each device keeps a table keyed by (log_n, log_blowup), log_blowup = 0 for
+ * the plain NTT; every entry point here uses the table's plan when present and
+ * the built-in one otherwise.  bc_autotune times every candidate plan on the
+ * current device (num_cols columns, reps timed runs after one warm-up; it
+ * allocates and frees its own scratch and synchronises) and stores the
+ * fastest; report (optional) receives one line per candidate. */
+cudaError_t bc_autotune(uint32_t log_n, uint32_t log_blowup, uint32_t num_cols, uint32_t reps, char *report,
+                        size_t report_len);
+/* Text form of the current device's table, one entry per line:
+ * "log_n log_blowup npasses K0 C0 [K1 C1 [K2 C2]]" (passes from the top bits). */
+cudaError_t bc_plan_table_export(char *buf, size_t len, size_t *needed);
+cudaError_t bc_plan_table_import(const char *text);
+cudaError_t bc_plan_table_clear(void);
+
 /* ---- coset low-degree extension ------------------------------------------
  * Input: num_cols columns of n = 2^log_n bit-reversed evaluations on the
  * subgroup H (column j at evals_bitrev + j * stride_in).  Output: for every
