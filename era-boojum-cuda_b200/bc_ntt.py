@@ -57,6 +57,7 @@ SIGNATURES = {
     "bc_lde_fused_profiled": [_vp, _vp, _u32, _u32, _u64, _u64, _u64, _u32, _vp, _vp, _u32, _vp],
     "bc_lde_host": [_vp, _vp, _u32, _u32, _u64, _u64, _u64, _u32, _vp, _sz, _u32, _vp],
     "bc_lde_batch_plan_create": [_vp, _u32, _vp],
+    "bc_lde_batch_plan_create_ex": [_vp, _u32, _u32, _vp],
     "bc_lde_batch_run": [_vp, _vp],
     "bc_lde_batch_status": [_vp, _vp, _vp],
     "bc_lde_batch_plan_info": [_vp, _vp, _vp, _vp],
@@ -207,9 +208,10 @@ def lde(evals_bitrev, out, log_n: int, num_cols: int, log_blowup: int, stride_in
 class LdeBatch:
     """A persistent-kernel batch plan over uneven LDE jobs (bc_lde_batch_*)."""
 
-    def __init__(self, jobs):
+    def __init__(self, jobs, standalone_min_ctas: int = 0):
         """jobs: list of (evals tensor, out tensor, log_n, num_cols, log_blowup) with dense coset-major outputs,
-        or LdeJob structures."""
+        or LdeJob structures.  standalone_min_ctas > 0: jobs whose kernels are at least that wide run as their own
+        kernels on a forked branch of the plan's graph (bc_lde_batch_plan_create_ex)."""
         arr = (LdeJob * max(1, len(jobs)))()
         for i, j in enumerate(jobs):
             if isinstance(j, LdeJob):
@@ -220,8 +222,8 @@ class LdeBatch:
                 arr[i] = LdeJob(_ptr(ev), _ptr(out), n, n, cols * n, log_n, cols, log_b, 0)
         self._jobs = arr
         self.handle = ctypes.c_void_p()
-        _check(lib().bc_lde_batch_plan_create(ctypes.cast(arr, _vp), len(jobs), ctypes.byref(self.handle)),
-               "bc_lde_batch_plan_create")
+        _check(lib().bc_lde_batch_plan_create_ex(ctypes.cast(arr, _vp), len(jobs), standalone_min_ctas,
+                                                 ctypes.byref(self.handle)), "bc_lde_batch_plan_create_ex")
 
     def run(self, stream=None):
         _check(lib().bc_lde_batch_run(self.handle, _stream(stream)), "bc_lde_batch_run")

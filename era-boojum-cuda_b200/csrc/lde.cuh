@@ -238,6 +238,9 @@ bool build_lde_steps(const Plan &pl, const uint64_t *in, uint64_t *out, uint32_t
 bool lde_args_ok(uint32_t log_n, uint32_t num_cols, uint64_t stride_in, uint64_t stride_out, uint64_t coset_stride,
                  uint32_t log_blowup);
 
+// Launches one step (pass or top-window kernel) on `stream`.
+cudaError_t launch_lde_step(const LdeStep &st, cudaStream_t stream);
+
 // Launches the fused LDE's kernels on `stream`; events (optional): ev[0] is
 // recorded before the first kernel and ev[j + 1] after kernel j.
 cudaError_t lde_fused(const Plan &pl, const uint64_t *in, uint64_t *out, uint32_t log_n, uint32_t num_cols,

@@ -182,8 +182,12 @@ cudaError_t free_plan(bc_lde_batch_plan *p) {
 uint64_t job_work(const bc_lde_job &j) { return ((uint64_t)j.num_cols << j.log_n) << j.log_blowup; }
 
 // Records and items of a batch, in dependency order (host side).
+// standalone_min_ctas > 0: a job whose every kernel, launched on its own, has
+// at least that many CTAs goes to `standalone` (its fused-LDE steps in order)
+// instead of the persistent kernel's schedule.
 cudaError_t schedule(const bc_lde_job *jobs, uint32_t n_jobs, std::vector<BatchRecord> &recs,
-                     std::vector<uint64_t> &items) {
+                     std::vector<uint64_t> &items, uint32_t standalone_min_ctas = 0,
+                     std::vector<LdeStep> *standalone = nullptr) {
   std::vector<std::vector<LdeStep>> steps(n_jobs);
   size_t max_depth = 0;
   for (uint32_t j = 0; j < n_jobs; j++) {
@@ -191,6 +195,18 @@ cudaError_t schedule(const bc_lde_job *jobs, uint32_t n_jobs, std::vector<BatchR
     if (!lde_args_ok(jb.log_n, jb.num_cols, jb.stride_in, jb.stride_out, jb.coset_stride, jb.log_blowup))
       return cudaErrorInvalidValue;
     if (jb.num_cols && (!jb.evals_bitrev || !jb.out)) return cudaErrorInvalidValue;
+    if (standalone_min_ctas && standalone && jb.num_cols) {
+      std::vector<LdeStep> own;
+      if (!build_lde_steps(tuned_plan(jb.log_n, jb.log_blowup), jb.evals_bitrev, jb.out, jb.log_n, jb.num_cols,
+                           jb.stride_in, jb.stride_out, jb.coset_stride, jb.log_blowup, false, 8, own))
+        return cudaErrorInvalidConfiguration;
+      uint64_t min_ctas = ~0ull;
+      for (const LdeStep &st : own) min_ctas = std::min<uint64_t>(min_ctas, (uint64_t)st.grid.x * st.grid.y);
+      if (min_ctas >= standalone_min_ctas) {
+        standalone->insert(standalone->end(), own.begin(), own.end());
+        continue; // steps[j] stays empty: no records for this job
+      }
+    }
     // the tuned plan, or the built-in one when the tuned plan uses a window shape this kernel does not carry
     auto build = [&](const Plan &pl) {
       if (!build_lde_steps(pl, jb.evals_bitrev, jb.out, jb.log_n, jb.num_cols, jb.stride_in, jb.stride_out,
@@ -241,13 +257,15 @@ cudaError_t schedule(const bc_lde_job *jobs, uint32_t n_jobs, std::vector<BatchR
 
 } // namespace
 
-extern "C" cudaError_t bc_lde_batch_plan_create(const bc_lde_job *jobs, uint32_t n_jobs, bc_lde_batch_plan **plan) {
+extern "C" cudaError_t bc_lde_batch_plan_create_ex(const bc_lde_job *jobs, uint32_t n_jobs,
+                                                   uint32_t standalone_min_ctas, bc_lde_batch_plan **plan) {
   if (!plan || (n_jobs && !jobs)) return cudaErrorInvalidValue;
   *plan = nullptr;
   if (!device_tables()) return cudaErrorInitializationError;
   std::vector<BatchRecord> recs;
   std::vector<uint64_t> items;
-  cudaError_t e = schedule(jobs, n_jobs, recs, items);
+  std::vector<LdeStep> standalone;
+  cudaError_t e = schedule(jobs, n_jobs, recs, items, standalone_min_ctas, &standalone);
   if (e != cudaSuccess) return e;
   bc_lde_batch_plan *p = new (std::nothrow) bc_lde_batch_plan();
   if (!p) return cudaErrorMemoryAllocation;
@@ -278,18 +296,36 @@ extern "C" cudaError_t bc_lde_batch_plan_create(const bc_lde_job *jobs, uint32_t
   }
   CK(cudaMalloc(&p->d_counters, (p->n_records + 2) * sizeof(uint32_t)));
   CK(cudaMemset(p->d_counters, 0, (p->n_records + 2) * sizeof(uint32_t)));
-  // capture: reset the counters, run the persistent kernel
-  cudaStream_t cs;
+  // capture: reset the counters, run the persistent kernel; the standalone jobs'
+  // kernels run on a forked branch of the same graph, concurrently with it
+  cudaStream_t cs, cs2;
+  cudaEvent_t fork, join;
   CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
-  e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+  CK(cudaStreamCreateWithFlags(&cs2, cudaStreamNonBlocking));
+  CK(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+  e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeRelaxed);
   if (e == cudaSuccess) {
-    cudaMemsetAsync(p->d_counters, 0, (p->n_records + 2) * sizeof(uint32_t), cs);
-    if (p->n_items)
+    cudaError_t ec = cudaMemsetAsync(p->d_counters, 0, (p->n_records + 2) * sizeof(uint32_t), cs);
+    if (ec == cudaSuccess && !standalone.empty()) {
+      ec = cudaEventRecord(fork, cs);
+      if (ec == cudaSuccess) ec = cudaStreamWaitEvent(cs2, fork, 0);
+      for (size_t i = 0; ec == cudaSuccess && i < standalone.size(); i++) ec = launch_lde_step(standalone[i], cs2);
+      if (ec == cudaSuccess) ec = cudaEventRecord(join, cs2);
+    }
+    if (ec == cudaSuccess && p->n_items) {
       lde_batch_kernel<<<p->grid, BATCH_THREADS, BATCH_SMEM_BYTES, cs>>>(
           p->d_records, p->d_items, p->n_items, p->d_counters, p->d_counters + p->n_records,
           p->d_counters + p->n_records + 1, p->timeout_cycles);
+      ec = cudaGetLastError();
+    }
+    if (ec == cudaSuccess && !standalone.empty()) ec = cudaStreamWaitEvent(cs, join, 0);
     e = cudaStreamEndCapture(cs, &p->graph);
+    if (e == cudaSuccess) e = ec;
   }
+  cudaEventDestroy(fork);
+  cudaEventDestroy(join);
+  cudaStreamDestroy(cs2);
   cudaStreamDestroy(cs);
   if (e != cudaSuccess) {
     free_plan(p);
@@ -299,6 +335,10 @@ extern "C" cudaError_t bc_lde_batch_plan_create(const bc_lde_job *jobs, uint32_t
 #undef CK
   *plan = p;
   return cudaSuccess;
+}
+
+extern "C" cudaError_t bc_lde_batch_plan_create(const bc_lde_job *jobs, uint32_t n_jobs, bc_lde_batch_plan **plan) {
+  return bc_lde_batch_plan_create_ex(jobs, n_jobs, 0, plan);
 }
 
 extern "C" cudaError_t bc_lde_batch_run(bc_lde_batch_plan *plan, cudaStream_t stream) {

@@ -173,6 +173,13 @@ typedef struct bc_lde_job {
 typedef struct bc_lde_batch_plan bc_lde_batch_plan;
 
 cudaError_t bc_lde_batch_plan_create(const bc_lde_job *jobs, uint32_t n_jobs, bc_lde_batch_plan **plan);
+/* Same, except that a job whose every fused-LDE kernel would launch at least
+ * standalone_min_ctas CTAs on its own is run as those kernels, on a branch of
+ * the plan's graph forked beside the persistent kernel that runs all other
+ * jobs (0: every job in the persistent kernel, as bc_lde_batch_plan_create).
+ * Big jobs gain nothing from sharing a launch; small ones do. */
+cudaError_t bc_lde_batch_plan_create_ex(const bc_lde_job *jobs, uint32_t n_jobs, uint32_t standalone_min_ctas,
+                                        bc_lde_batch_plan **plan);
 cudaError_t bc_lde_batch_run(bc_lde_batch_plan *plan, cudaStream_t stream);
 /* Waits for the stream, then returns the status word of the plan's last run. */
 cudaError_t bc_lde_batch_status(bc_lde_batch_plan *plan, cudaStream_t stream, uint32_t *status);

@@ -115,3 +115,24 @@ def test_batch_empty_and_single(gpu_ctx):
     assert plan.status() == 0
     np.testing.assert_array_equal(to_host(out), oracle.lde(x, 12, 1, 1 << 12, 1))
     plan.close()
+
+
+def test_hybrid_plan_standalone_big_jobs(gpu_ctx):
+    """Big jobs as their own kernels on a forked graph branch, small ones in the persistent kernel: exact."""
+    import bc_ntt
+    import torch
+
+    rng = np.random.default_rng(77)
+    jobs = _mixed_jobs(rng, SPECS)
+    for min_ctas in (64, 1):  # a mix of both paths, then every job standalone
+        for ev, out, *_ in jobs:
+            out.fill_(0)
+        plan = bc_ntt.LdeBatch([j[:5] for j in jobs], standalone_min_ctas=min_ctas)
+        plan.run()
+        assert plan.status() == 0
+        for ev, out, log_n, cols, log_b, x in jobs:
+            ref = torch.empty_like(out)
+            bc_ntt.lde(ev, ref, log_n, cols, log_b, fused=True)
+            torch.cuda.synchronize()
+            assert torch.equal(out, ref), f"min_ctas={min_ctas} log_n={log_n} cols={cols}"
+        plan.close()
