@@ -135,14 +135,22 @@ def dist_setup(gpus: int):
 
 
 def barrier_max(value: float, world: int) -> float:
+    """Max of a per-rank value over all ranks (the job's time is its slowest rank's)."""
     if world == 1:
         return value
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([value], device="cuda", dtype=torch.float64)
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], device=dev, dtype=torch.float64)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def whole_job_value(world: int, steps: int, units_per_rank_step: int, max_total_ms: float) -> float:
+    """Whole-job throughput in M units/s: every rank processes its own units (weak scaling), the time is
+    the max over ranks of the timed region."""
+    return world * steps * units_per_rank_step / (max_total_ms / 1e3) / 1e6
 
 
 def barrier(world: int):
@@ -255,7 +263,7 @@ def run_ours(args, rank, world):
     plain_ms, plain_per = time_steps(plain, max(3, args.steps // 2), 1, world, stream)
 
     out_elems = B * n * COLS
-    value = world * args.steps * out_elems / (total_ms / 1e3) / 1e6
+    value = whole_job_value(world, args.steps, out_elems, total_ms)
     ms_per_step = total_ms / args.steps
 
     # dominant kernel: per-kernel durations from events recorded between the fused LDE's launches
@@ -606,7 +614,7 @@ def run_reference(args, rank, world):
     with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
         total_ms, per = time_steps(step, args.steps, args.warmup, world, stream)
     out_elems = B * n * COLS
-    value = world * args.steps * out_elems / (total_ms / 1e3) / 1e6
+    value = whole_job_value(world, args.steps, out_elems, total_ms)
     hx = torch.empty(COLS * n, dtype=torch.int64, pin_memory=True)
     hx.copy_(x)
     hout = torch.empty(B * COLS * n, dtype=torch.int64, pin_memory=True)
