@@ -102,12 +102,164 @@ __device__ __forceinline__ uint64_t reduce128(uint64_t lo, uint64_t hi) {
   return r;
 }
 
-__device__ __forceinline__ uint64_t mul(uint64_t a, uint64_t b) { return reduce128(a * b, __umul64hi(a, b)); }
-
-__device__ __forceinline__ uint64_t sqr(uint64_t a) { return mul(a, a); }
-
 // Canonical representative in [0, p).
 __device__ __forceinline__ uint64_t canon(uint64_t x) { return x >= P ? x - P : x; }
+
+__device__ __forceinline__ uint64_t mul(uint64_t a, uint64_t b) { return reduce128(a * b, __umul64hi(a, b)); }
+
+// a + b (mod p) for b < p: a + b < 2^64 + p, so one carry correction suffices.
+__device__ __forceinline__ uint64_t add_bc(uint64_t a, uint64_t b) {
+  uint64_t r;
+  asm("{\n\t"
+      ".reg .u32 a0, a1, b0, b1, r0, r1, c;\n\t"
+      "mov.b64 {a0, a1}, %1;\n\t"
+      "mov.b64 {b0, b1}, %2;\n\t"
+      "add.cc.u32 r0, a0, b0;\n\t"
+      "addc.cc.u32 r1, a1, b1;\n\t"
+      "addc.u32 c, 0, 0;\n\t"
+      "neg.s32 c, c;\n\t"
+      "add.cc.u32 r0, r0, c;\n\t"
+      "addc.u32 r1, r1, 0;\n\t"
+      "mov.b64 %0, {r0, r1};\n\t"
+      "}"
+      : "=l"(r)
+      : "l"(a), "l"(b));
+  return r;
+}
+
+// a - b (mod p) for b < p: a - b > -p, so one borrow correction suffices.
+__device__ __forceinline__ uint64_t sub_bc(uint64_t a, uint64_t b) {
+  uint64_t r;
+  asm("{\n\t"
+      ".reg .u32 a0, a1, b0, b1, r0, r1, c;\n\t"
+      "mov.b64 {a0, a1}, %1;\n\t"
+      "mov.b64 {b0, b1}, %2;\n\t"
+      "sub.cc.u32 r0, a0, b0;\n\t"
+      "subc.cc.u32 r1, a1, b1;\n\t"
+      "subc.u32 c, 0, 0;\n\t"
+      "sub.cc.u32 r0, r0, c;\n\t"
+      "subc.u32 r1, r1, 0;\n\t"
+      "mov.b64 %0, {r0, r1};\n\t"
+      "}"
+      : "=l"(r)
+      : "l"(a), "l"(b));
+  return r;
+}
+
+// lo + h * EPS (mod p) for h < 2^32.  h * EPS = (h << 32) - h <= 2^64 - 2^33 + 1
+// needs no reduction, and s = lo + h * EPS carries at most once.  After a
+// carry, s - 2^64 + EPS < h * EPS + EPS <= p - 1 is already canonical; without
+// one, s >= p exactly when s + EPS carries, and then s + EPS - 2^64 = s - p.
+// CANON selects that canonical result; otherwise the carry is folded back as
+// EPS and the result is only < 2^64.
+template <bool CANON>
+__device__ __forceinline__ uint64_t add_h_eps(uint64_t lo, uint32_t h) {
+  uint64_t r;
+  if constexpr (CANON) {
+    asm("{\n\t"
+        ".reg .u32 l0, l1, u0, u1, v0, v1, c;\n\t"
+        ".reg .pred q;\n\t"
+        "mov.b64 {l0, l1}, %1;\n\t"
+        "sub.cc.u32 u0, 0, %2;\n\t"
+        "subc.u32 u1, %2, 0;\n\t"
+        "add.cc.u32 l0, l0, u0;\n\t"
+        "addc.cc.u32 l1, l1, u1;\n\t"
+        "addc.u32 c, 0, 0;\n\t"
+        "add.cc.u32 v0, l0, 0xffffffff;\n\t"
+        "addc.cc.u32 v1, l1, 0;\n\t"
+        "addc.u32 c, c, 0;\n\t"
+        "setp.ne.u32 q, c, 0;\n\t"
+        "selp.b32 l0, v0, l0, q;\n\t"
+        "selp.b32 l1, v1, l1, q;\n\t"
+        "mov.b64 %0, {l0, l1};\n\t"
+        "}"
+        : "=l"(r)
+        : "l"(lo), "r"(h));
+  } else {
+    asm("{\n\t"
+        ".reg .u32 l0, l1, u0, u1, c;\n\t"
+        "mov.b64 {l0, l1}, %1;\n\t"
+        "sub.cc.u32 u0, 0, %2;\n\t"
+        "subc.u32 u1, %2, 0;\n\t"
+        "add.cc.u32 l0, l0, u0;\n\t"
+        "addc.cc.u32 l1, l1, u1;\n\t"
+        "addc.u32 c, 0, 0;\n\t"
+        "neg.s32 c, c;\n\t"
+        "add.cc.u32 l0, l0, c;\n\t"
+        "addc.u32 l1, l1, 0;\n\t"
+        "mov.b64 %0, {l0, l1};\n\t"
+        "}"
+        : "=l"(r)
+        : "l"(lo), "r"(h));
+  }
+  return r;
+}
+
+// x * 2^E (mod p) for a compile-time 0 < E < 96 and any u64 x, without a
+// multiply.  x << E spans at most 160 bits, words v0..v4 (32 bits each), and
+//   v = v0 + v1 2^32 + v2 2^64 + v3 2^96 + v4 2^128
+//     = v0 - v2 - v3 + (v1 + v2 - v4) 2^32        (2^64 = 2^32 - 1, 2^96 = -1)
+// of which at most three words are non-zero for a given E.
+//   E < 32:       v = lo + h EPS, lo = x << E (64 bits), h = x >> (64 - E);
+//   32 <= E < 64: (v1 + v2) 2^32 - (v2 + v3), s = E - 32;
+//   64 <= E < 96: (v2 - v4) 2^32 - (v2 + v3), s = E - 64.
+// CANON: the result is reduced to [0, p).
+template <int E, bool CANON = false>
+__device__ __forceinline__ uint64_t mul_pow2(uint64_t x) {
+  static_assert(E > 0 && E < 96, "mul_pow2: 0 < E < 96");
+  if constexpr (E < 32) {
+    return add_h_eps<CANON>(x << E, (uint32_t)(x >> (64 - E)));
+  } else if constexpr (E < 64) {
+    constexpr int s = E - 32;
+    const uint64_t xs = x << s;
+    const uint32_t v1 = (uint32_t)xs, v2 = (uint32_t)(xs >> 32), v3 = s ? (uint32_t)(x >> (64 - s)) : 0u;
+    uint64_t r;
+    // S = v1 + v2 (carry c1: S 2^32 = S_lo 2^32 + c1 EPS), D = v2 + v3, r = S 2^32 - D
+    asm("{\n\t"
+        ".reg .u32 sl, m1, dl, c2, r0, r1, b;\n\t"
+        "add.cc.u32 sl, %1, %2;\n\t"
+        "addc.u32 m1, 0, 0;\n\t"
+        "neg.s32 m1, m1;\n\t"
+        "add.cc.u32 dl, %2, %3;\n\t"
+        "addc.u32 c2, 0, 0;\n\t"
+        "sub.cc.u32 r0, m1, dl;\n\t"
+        "subc.cc.u32 r1, sl, c2;\n\t"
+        "subc.u32 b, 0, 0;\n\t"
+        "sub.cc.u32 r0, r0, b;\n\t"
+        "subc.u32 r1, r1, 0;\n\t"
+        "mov.b64 %0, {r0, r1};\n\t"
+        "}"
+        : "=l"(r)
+        : "r"(v1), "r"(v2), "r"(v3));
+    return CANON ? canon(r) : r;
+  } else {
+    constexpr int s = E - 64;
+    const uint64_t xs = x << s;
+    const uint32_t y0 = (uint32_t)xs, y1 = (uint32_t)(xs >> 32), y2 = s ? (uint32_t)(x >> (64 - s)) : 0u;
+    uint64_t r;
+    // S = y0 - y2 (borrow: S 2^32 = S_lo 2^32 - EPS), D = y0 + y1 (+ EPS on that borrow), r = S_lo 2^32 - D
+    asm("{\n\t"
+        ".reg .u32 sl, m, dl, dh, r0, r1, b;\n\t"
+        "sub.cc.u32 sl, %1, %3;\n\t"
+        "subc.u32 m, 0, 0;\n\t"
+        "add.cc.u32 dl, %1, %2;\n\t"
+        "addc.u32 dh, 0, 0;\n\t"
+        "add.cc.u32 dl, dl, m;\n\t"
+        "addc.u32 dh, dh, 0;\n\t"
+        "sub.cc.u32 r0, 0, dl;\n\t"
+        "subc.cc.u32 r1, sl, dh;\n\t"
+        "subc.u32 b, 0, 0;\n\t"
+        "sub.cc.u32 r0, r0, b;\n\t"
+        "subc.u32 r1, r1, 0;\n\t"
+        "mov.b64 %0, {r0, r1};\n\t"
+        "}"
+        : "=l"(r)
+        : "r"(y0), "r"(y1), "r"(y2));
+    return CANON ? canon(r) : r;
+  }
+}
+
+__device__ __forceinline__ uint64_t sqr(uint64_t a) { return mul(a, a); }
 
 __device__ __forceinline__ uint64_t pow(uint64_t b, uint32_t e) {
   uint64_t r = 1;

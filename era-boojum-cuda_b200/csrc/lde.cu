@@ -163,7 +163,9 @@ bool build_lde_steps(const Plan &pl, const uint64_t *in, uint64_t *out, uint32_t
     p.tabs = *tabs;
     const uint32_t tile = G << wc_log;
     st.threads = tile / 16;
-    st.smem = (size_t)top_smem_words(tile, K) * sizeof(uint64_t);
+    const uint32_t nb = 1u << log_blowup;
+    p.fwd_resident = (size_t)top_smem_words(tile, K, nb) * sizeof(uint64_t) <= TOP_RESIDENT_SMEM_MAX ? 1 : 0;
+    st.smem = (size_t)top_smem_words(tile, K, p.fwd_resident ? nb : 1) * sizeof(uint64_t);
     const uint64_t gy = (num_cols + p.cols_per_cta - 1) / p.cols_per_cta;
     if (gy > 65535 || tiles > 0x7fffffffull) return false;
     st.grid = dim3((uint32_t)tiles, (uint32_t)gy);

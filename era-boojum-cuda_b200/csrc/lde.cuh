@@ -27,6 +27,7 @@ struct LdeTopParams {
   uint32_t cols_per_cta;
   uint32_t canon_out; // single-pass plan: this kernel writes final values
   uint32_t vec_in, vec_out;
+  uint32_t fwd_resident; // the forward power tables of all cosets stay in shared memory
   DevTables tabs;
 };
 
@@ -69,18 +70,25 @@ __device__ __forceinline__ void top_body(const LdeTopParams &p, uint32_t bx, uin
   const uint32_t TILE = G * W * C;
   const uint32_t T = TILE / 16;
   uint64_t *tile = smem;
-  uint64_t *tws_inv = smem + TILE + TILE / 16;
-  uint64_t *tws_fwd = tws_inv + TwSlots<K>::words;
+  // power tables (ntt_pass.cuh): the inverse one, then one forward table per
+  // coset (fwd_resident, filled once per CTA) or one refilled for every coset
+  uint64_t *pw_inv = smem + TILE + TILE / 16;
+  uint64_t *pw_fwd = pw_inv + PowWords<K>::words;
   const uint32_t tid = threadIdx.x;
 
   // top window: H = 0, the tile position is the run of low positions
   const uint64_t base_off = (uint64_t)bx << LogC<C>::v;
   const uint32_t col_begin = by * p.cols_per_cta;
   const uint32_t col_end = min(p.num_cols, col_begin + p.cols_per_cta);
-  fill_twiddles<K>(tws_inv, p.tabs, 1, 0, tid, T);
+  fill_powers<K>(pw_inv, p.tabs, 1, 0, tid, T);
+  const uint32_t nb = 1u << p.log_blowup;
+  if (p.fwd_resident)
+    for (uint32_t k = 0; k < nb; k++)
+      fill_powers<K>(pw_fwd + k * PowWords<K>::words, p.tabs, 0, brev_bits(k, p.log_blowup), tid, T,
+                     (k + 1) * PowWords<K>::tasks);
+  // the column loop's first barrier orders these fills before any use
 
   const uint64_t inv_n = p.tabs.inv_pow2[p.log_n];
-  const uint32_t nb = 1u << p.log_blowup;
 
   for (uint32_t c0 = col_begin; c0 < col_end; c0 += G) {
 #pragma unroll
@@ -112,7 +120,7 @@ __device__ __forceinline__ void top_body(const LdeTopParams &p, uint32_t bx, uin
       using S = RoundShape<K, false, false, 0>;
       uint64_t coef[16];
       load_groups<K, C, S::B, S::V>(tile, coef, tid, T);
-      compute_groups<K, C, true, S::B, S::V>(coef, tws_inv, tid, T);
+      compute_groups<K, C, true, true, S::B, S::V>(coef, pw_inv, tid, T);
       constexpr int NV = 1 << S::V, NG = 16 / NV;
 #pragma unroll
       for (int q = 0; q < NG; q++) {
@@ -130,20 +138,24 @@ __device__ __forceinline__ void top_body(const LdeTopParams &p, uint32_t bx, uin
       }
       for (uint32_t k = 0; k < nb; k++) {
         __syncthreads();
-        fill_twiddles<K>(tws_fwd, p.tabs, 0, brev_bits(k, p.log_blowup), tid, T);
-        __syncthreads();
+        const uint64_t *pwk = pw_fwd + (p.fwd_resident ? k * PowWords<K>::words : 0);
+        if (!p.fwd_resident) {
+          fill_powers<K>(pw_fwd, p.tabs, 0, brev_bits(k, p.log_blowup), tid, T);
+          __syncthreads();
+        }
         uint64_t x[16];
 #pragma unroll
         for (int j = 0; j < 16; j++) x[j] = coef[j];
-        compute_groups<K, C, false, S::B, S::V>(x, tws_fwd, tid, T);
+        compute_groups<K, C, false, false, S::B, S::V>(x, pwk, tid, T);
         store_groups<K, C, S::B, S::V>(tile, x, tid, T);
         __syncthreads();
         top_store(p, tile, c0, col_end, k, base_off, tid, T);
       }
     } else {
       // inverse stages of the window (bottom-up): the short round first, then the
-      // full rounds; the last full round (top 4 bits) stays in registers, scaled
-      if constexpr (R > 0) rounds_from<K, C, true, true, 0, 1>(tile, tws_inv, tid, T);
+      // full rounds; the last full round (top 4 bits, R = 0: no powers) stays in
+      // registers, scaled
+      if constexpr (R > 0) rounds_from<K, C, true, true, true, 0, 1>(tile, pw_inv, tid, T);
       uint32_t w;
       const uint32_t eb = gbase16<K, C>(tid, K - 4, w);
       uint64_t coef[16];
@@ -157,7 +169,7 @@ __device__ __forceinline__ void top_body(const LdeTopParams &p, uint32_t bx, uin
         uint64_t x[16];
 #pragma unroll
         for (int j = 0; j < 16; j++) x[j] = tile[a[j]];
-        net16<K, true>(x, tws_inv, wr, B);
+        net16<K, true, true>(x, pw_inv, wr, B, r + 1 < NF);
         if (r + 1 < NF) {
 #pragma unroll
           for (int j = 0; j < 16; j++) tile[a[j]] = x[j];
@@ -179,10 +191,14 @@ __device__ __forceinline__ void top_body(const LdeTopParams &p, uint32_t bx, uin
         }
       }
       for (uint32_t k = 0; k < nb; k++) {
-        __syncthreads(); // previous coset's stores have read the tile and twiddles
-        fill_twiddles<K>(tws_fwd, p.tabs, 0, brev_bits(k, p.log_blowup), tid, T);
-        __syncthreads();
+        __syncthreads(); // previous coset's stores have read the tile (and the powers)
+        const uint64_t *pwk = pw_fwd + (p.fwd_resident ? k * PowWords<K>::words : 0);
+        if (!p.fwd_resident) {
+          fill_powers<K>(pw_fwd, p.tabs, 0, brev_bits(k, p.log_blowup), tid, T);
+          __syncthreads();
+        }
         // forward stages (top-down): the first full round starts from the registers
+        // (its R is the coset prefix brev(k): s = 1 for k = 0)
 #pragma unroll 1
         for (int r = 0; r < NF; r++) {
           const uint32_t B = (uint32_t)(K - 4 - 4 * r);
@@ -198,12 +214,12 @@ __device__ __forceinline__ void top_body(const LdeTopParams &p, uint32_t bx, uin
 #pragma unroll
             for (int j = 0; j < 16; j++) x[j] = tile[a[j]];
           }
-          net16<K, false>(x, tws_fwd, wr, B);
+          net16<K, false, false>(x, pwk, wr, B, r > 0 || k != 0);
 #pragma unroll
           for (int j = 0; j < 16; j++) tile[a[j]] = x[j];
           __syncthreads();
         }
-        if constexpr (R > 0) rounds_from<K, C, false, false, NF>(tile, tws_fwd, tid, T);
+        if constexpr (R > 0) rounds_from<K, C, false, false, false, NF>(tile, pwk, tid, T);
         top_store(p, tile, c0, col_end, k, base_off, tid, T);
       }
     }
@@ -211,9 +227,16 @@ __device__ __forceinline__ void top_body(const LdeTopParams &p, uint32_t bx, uin
   }
 }
 
-__host__ __device__ constexpr uint32_t top_smem_words(uint32_t tile, int K) {
-  return tile + tile / 16 + 2 * ((1u << K) + (1u << K) / 16);
+// Shared memory (u64 words) of top_body: tile, padding, the inverse power
+// table and fwd_tables forward ones.
+__host__ __device__ constexpr uint32_t top_smem_words(uint32_t tile, int K, uint32_t fwd_tables) {
+  return tile + tile / 16 + (1 + fwd_tables) * (1u << K);
 }
+
+// Largest shared memory of a top-window kernel whose forward tables stay
+// resident: that of a 4096-element tile of 12 bits with one forward table
+// (98 KB), which keeps two CTAs on an SM and fits the persistent kernel.
+constexpr uint32_t TOP_RESIDENT_SMEM_MAX = top_smem_words(4096, 12, 1) * 8;
 
 // One kernel of a fused LDE: either a pass (ntt_pass_kernel) or the top-window
 // kernel, with its parameters and launch shape.

@@ -57,7 +57,7 @@ __host__ __device__ constexpr uint64_t make_item(uint32_t rec, uint32_t by, uint
 }
 
 constexpr uint32_t BATCH_THREADS = 256;
-constexpr uint32_t BATCH_SMEM_BYTES = top_smem_words(4096, 12) * 8; // largest body: top window of 12 bits
+constexpr uint32_t BATCH_SMEM_BYTES = TOP_RESIDENT_SMEM_MAX; // largest body: top window of 12 bits, one forward table
 
 // The bodies the persistent kernel can run: every window shape of the default
 // plans (and of the tuner's candidates).
@@ -84,7 +84,7 @@ __device__ __noinline__ void run_shape(const BatchRecord &rec, uint32_t bx, uint
   if constexpr (TOP)
     top_body<K, C>(rec.u.top, bx, by, smem);
   else
-    pass_body<K, C, B2N>(rec.u.pass, bx, by, smem);
+    pass_body<K, C, B2N, B2N>(rec.u.pass, bx, by, smem); // LDE passes: b2n ones are the inverse transform
 }
 
 __device__ __forceinline__ void run_body(const BatchRecord &rec, uint32_t bx, uint32_t by, uint64_t *smem) {
@@ -214,7 +214,8 @@ cudaError_t schedule(const bc_lde_job *jobs, uint32_t n_jobs, std::vector<BatchR
         return false;
       for (const LdeStep &st : steps[j])
         if (!batch_shape_supported(shape_id(st.top, st.b2n, st.K, st.C)) || st.threads != BATCH_THREADS ||
-            st.smem > BATCH_SMEM_BYTES || st.grid.x >= (1u << 28) || st.grid.y >= (1u << 20))
+            st.smem > BATCH_SMEM_BYTES || st.grid.x >= (1u << 28) || st.grid.y >= (1u << 20) ||
+            (!st.top && st.pass.inverse != (uint32_t)st.b2n)) // the kernel carries LDE passes only
           return false;
       return true;
     };

@@ -122,6 +122,10 @@ cudaError_t context_create_current() {
   std::vector<uint64_t> h;
   size_t off[12];
   build_host_tables(h, off);
+  // the pass kernels apply T[u], u < 8, as shifts by small_tw_exp
+  for (int inv_ = 0; inv_ < 2; inv_++)
+    for (int u = 0; u < 8; u++)
+      if (h[off[0 + inv_] + u] != hostf::pow(2, (uint64_t)small_tw_exp(inv_ != 0, u))) return cudaErrorInvalidValue;
   cudaError_t e = cudaMalloc(&c.block, TABLE_WORDS * sizeof(uint64_t));
   if (e != cudaSuccess) return e;
   e = cudaMemcpy(c.block, h.data(), TABLE_WORDS * sizeof(uint64_t), cudaMemcpyHostToDevice);

@@ -21,7 +21,9 @@
 // with coalesced 16-byte accesses into padded shared memory (one pad word
 // every 16 words keeps the strided radix-16 accesses conflict-free), then
 // processed in rounds of up to 4 stages held in registers (16 values per
-// thread), then stored.  The 2^K - 1 twiddles a tile position needs are
+// thread), then stored.  A round multiplies by powers s^j of one twiddle per
+// group and then runs a fixed network of shift multiplications (see the
+// factored rounds below); the 2^K - 1 powers a tile position needs are
 // computed once per CTA into shared memory and reused for all its columns.
 //
 // Column groups.  Columns may come in 2^log_groups groups (group k at
@@ -106,24 +108,36 @@ __device__ __forceinline__ uint32_t pad16(uint32_t x) { return x + (x >> 4); }
 
 __device__ __forceinline__ uint32_t brev_bits(uint32_t x, uint32_t bits) { return bits ? __brev(x) >> (32 - bits) : 0; }
 
-__device__ __forceinline__ void dit(uint64_t &a, uint64_t &b, uint64_t t) {
-  const uint64_t bt = gl::mul(b, t);
-  const uint64_t a0 = a;
-  a = gl::add(a0, bt);
-  b = gl::sub(a0, bt);
-}
+// ---------------------------------------------------------------- factored rounds
+// A round holds V window bits [B, B + V) of 16 / 2^V groups per thread in
+// registers: x[q * 2^V + j] is element j of the thread's q-th group (j is the
+// value of the round's bits, its top bit the round's top stage bit).
+//
+// Factoring.  In a round, the pair of stage bit a = B + qq uses
+// T[(R << (V-1-qq)) + u]: R = idx >> (B + V) is the upper part of the group
+// (one value for its 2^V elements) and u = j >> (qq + 1) < 2^(V-1-qq) are the
+// round bits above a.  Bit-reversed twiddles multiply over disjoint bit fields,
+// T[(R << m) + u] = T[R << m] T[u], and T[2r]^2 = T[r] gives
+// T[R << m] = s^(2^(V-1-m)) with s = T[R << (V-1)].  A DIT round is therefore
+//     x_j <- x_j s^j  (j = 1 .. 2^V - 1),  then the same network with R = 0,
+// and a DIF round (its inverse, stage by stage, with the inverse table) is the
+// R = 0 network followed by x_j <- x_j s^j.  The R = 0 network's twiddles
+// T[u], u < 8, are signed powers of two (small_tw_exp), applied with shifts
+// (gl::mul_pow2): a round costs 2^V - 1 general multiplications instead of
+// V 2^(V-1), plus shift multiplications.  A DIT butterfly by -2^e swaps its
+// sum and difference; a DIF one swaps the operands of its difference.
+//
+// Power table of one tile position.  The window's rounds partition its bits
+// into full rounds [K - 4(i+1), K - 4i) from the top and a short round
+// [0, K mod 4).  The round on [B, B + V) has NR = 2^(K-B-V) values of
+// R_local (the window bits above it; R = (H << (K-B-V)) + R_local) and keeps
+// s^j of R_local at entry (NR - 1) + R_local (2^V - 1) + j - 1: the rounds
+// above it hold exactly NR - 1 entries, and the table 2^K - 1.  The odd
+// stride 2^V - 1 keeps a half-warp's reads of distinct R_local on distinct
+// banks.
 
-__device__ __forceinline__ void dif(uint64_t &a, uint64_t &b, uint64_t t) {
-  const uint64_t a0 = a;
-  a = gl::add(a0, b);
-  b = gl::mul(gl::sub(a0, b), t);
-}
-
-// ---------------------------------------------------------------- rounds
-// A round holds the V window bits [B, B + V) of 16 / 2^V groups per thread in
-// registers: x[q * 2^V + j] is element j of the thread's q-th group.
-
-// Which index runs fastest across consecutive threads of a round.  Runs of C
+// Tile index of element 0 of group gi, and its window value w (bits [B, B+V) zero).
+// Which index runs fastest across consecutive threads of a round: runs of C
 // low positions first keeps a half-warp on 16 distinct banks for every full
 // round; a short round on the window's bottom bits with C > 1 instead needs
 // the other window bits first (group stride 2^V * C <= 16 words).
@@ -131,7 +145,6 @@ template <int C, int B, int V> struct GroupOrder {
   static constexpr bool window_first = (V < 4) && (B == 0) && (C > 1) && ((1 << V) * C <= 16);
 };
 
-// Tile index of element 0 of group gi, and its window value w (bits [B, B+V) zero).
 template <int K, int C, int B, int V>
 __device__ __forceinline__ uint32_t group_base(uint32_t gi, uint32_t &w) {
   constexpr int W = 1 << K;
@@ -175,43 +188,6 @@ __device__ __forceinline__ void store_groups(uint64_t *tile, const uint64_t (&x)
   }
 }
 
-// Shared-memory twiddle slot of entry i: level L (2^L entries) starts at 2^L
-// (entry 0 unused) and one pad word follows every 16, which keeps every
-// round's twiddle reads on distinct banks.
-__device__ __forceinline__ uint32_t tw_slot(uint32_t i) { return i + (i >> 4); }
-template <int K> struct TwSlots {
-  static constexpr uint32_t words = (1u << K) + (1u << K) / 16;
-};
-
-// Stages of one round.  DIF: bottom bit first, (a+b, (a-b)t); DIT: top bit
-// first, (a+bt, a-bt).  Twiddle of window bit qb for upper window part u:
-// entry 2^(K-1-qb) + u of the tile's twiddle table.
-template <int K, int C, bool DIF, int B, int V>
-__device__ __forceinline__ void compute_groups(uint64_t (&x)[16], const uint64_t *tws, uint32_t tid,
-                                               uint32_t nthreads) {
-  constexpr int NV = 1 << V, NG = 16 / NV;
-#pragma unroll
-  for (int q = 0; q < NG; q++) {
-    uint32_t w;
-    group_base<K, C, B, V>(tid + nthreads * q, w);
-#pragma unroll
-    for (int s = 0; s < V; s++) {
-      const int qq = DIF ? s : V - 1 - s;
-      const int qb = B + qq;
-#pragma unroll
-      for (int j0 = 0; j0 < NV; j0++) {
-        if (j0 & (1 << qq)) continue;
-        const uint32_t u = (w | ((uint32_t)j0 << B)) >> (qb + 1);
-        const uint64_t t = tws[tw_slot((1u << (K - 1 - qb)) + u)];
-        if (DIF)
-          dif(x[q * NV + j0], x[q * NV + (j0 | (1 << qq))], t);
-        else
-          dit(x[q * NV + j0], x[q * NV + (j0 | (1 << qq))], t);
-      }
-    }
-  }
-}
-
 // Round ri of K window bits.  DIT rounds run top-down with the short round
 // last; DIF rounds run bottom-up, short round last or (RAGGED_FIRST) first.
 template <int K, bool DIF, bool RAGGED_FIRST, int RI> struct RoundShape {
@@ -224,31 +200,134 @@ template <int K, bool DIF, bool RAGGED_FIRST, int RI> struct RoundShape {
   static constexpr int NR = (K + 3) / 4;
 };
 
+// Words of a tile position's power table, and its fill tasks (R_local values
+// over all rounds).
+template <int K> struct PowWords {
+  static constexpr uint32_t words = 1u << K;
+  static constexpr uint32_t tasks = ((1u << (4 * (K / 4))) - 1) / 15 + (K % 4 ? (1u << (K - K % 4)) : 0);
+};
+
+// Powers s^1 .. s^(2^V - 1) of every R_local of the round on [B, B + V).
+// Tasks start at thread `first` so that consecutive rounds use different threads.
+template <int K, int B, int V>
+__device__ __forceinline__ void fill_round_powers(uint64_t *pw, const DevTables &tabs, uint32_t inv, uint32_t H,
+                                                  uint32_t first, uint32_t tid, uint32_t nthreads) {
+  constexpr uint32_t NR = 1u << (K - B - V);
+  constexpr int NP = (1 << V) - 1;
+  uint64_t *base = pw + (NR - 1);
+  for (uint32_t r = (tid + nthreads - first) % nthreads; r < NR; r += nthreads) {
+    uint64_t sp[NP + 1];
+    sp[1] = twiddle(tabs, inv, (H << (K - B - 1)) + (r << (V - 1)));
+#pragma unroll
+    for (int j = 2; j <= NP; j++) sp[j] = (j & 1) ? gl::mul(sp[j - 1], sp[1]) : gl::sqr(sp[j / 2]);
+#pragma unroll
+    for (int j = 1; j <= NP; j++) base[r * NP + j - 1] = sp[j];
+  }
+}
+
+// The power table of tile position H (window bits above the window, group
+// prefix included) for the forward (inv = 0) or inverse (inv = 1) twiddles.
+template <int K, int RI = 0>
+__device__ __forceinline__ void fill_powers(uint64_t *pw, const DevTables &tabs, uint32_t inv, uint32_t H,
+                                            uint32_t tid, uint32_t nthreads, uint32_t first = 0) {
+  using S = RoundShape<K, false, false, RI>;
+  if constexpr (RI < S::NR) {
+    fill_round_powers<K, S::B, S::V>(pw, tabs, inv, H, first % nthreads, tid, nthreads);
+    fill_powers<K, RI + 1>(pw, tabs, inv, H, tid, nthreads, first + (1u << (K - S::B - S::V)));
+  }
+}
+
+// Butterflies by the constant twiddle 2^E (E < 192).  DIT: the product is
+// reduced to [0, p), so the sum and difference need one correction each.
+template <int E> __device__ __forceinline__ void cdit(uint64_t &a, uint64_t &b) {
+  const uint64_t a0 = a;
+  if constexpr (E == 0) {
+    a = gl::add(a0, b);
+    b = gl::sub(a0, b);
+  } else if constexpr (E < 96) {
+    const uint64_t m = gl::mul_pow2<E, true>(b);
+    a = gl::add_bc(a0, m);
+    b = gl::sub_bc(a0, m);
+  } else {
+    const uint64_t m = gl::mul_pow2<E - 96, true>(b);
+    a = gl::sub_bc(a0, m);
+    b = gl::add_bc(a0, m);
+  }
+}
+
+template <int E> __device__ __forceinline__ void cdif(uint64_t &a, uint64_t &b) {
+  const uint64_t a0 = a;
+  a = gl::add(a0, b);
+  if constexpr (E == 0)
+    b = gl::sub(a0, b);
+  else if constexpr (E < 96)
+    b = gl::mul_pow2<E>(gl::sub(a0, b));
+  else
+    b = gl::mul_pow2<E - 96>(gl::sub(b, a0));
+}
+
+// One stage (bit QQ of a V-bit round) of the R = 0 network on x[OFF .. OFF + 2^V).
+template <bool DIF, bool INV, int V, int OFF, int QQ, int J0 = 0>
+__device__ __forceinline__ void cstage(uint64_t (&x)[16]) {
+  if constexpr (J0 < (1 << V)) {
+    if constexpr (!(J0 & (1 << QQ))) {
+      constexpr int E = small_tw_exp(INV, J0 >> (QQ + 1));
+      if constexpr (DIF)
+        cdif<E>(x[OFF + J0], x[OFF + (J0 | (1 << QQ))]);
+      else
+        cdit<E>(x[OFF + J0], x[OFF + (J0 | (1 << QQ))]);
+    }
+    cstage<DIF, INV, V, OFF, QQ, J0 + 1>(x);
+  }
+}
+
+// The R = 0 network of a V-bit round: DIT top bit first, DIF bottom bit first.
+template <bool DIF, bool INV, int V, int OFF, int S = 0>
+__device__ __forceinline__ void cnet(uint64_t (&x)[16]) {
+  if constexpr (S < V) {
+    cstage<DIF, INV, V, OFF, DIF ? S : V - 1 - S>(x);
+    cnet<DIF, INV, V, OFF, S + 1>(x);
+  }
+}
+
+// x[OFF + j] *= pp[j - 1] for j = 1 .. 2^V - 1.
+template <int V, int OFF>
+__device__ __forceinline__ void mul_powers(uint64_t (&x)[16], const uint64_t *pp) {
+#pragma unroll
+  for (int j = 1; j < (1 << V); j++) x[OFF + j] = gl::mul(x[OFF + j], pp[j - 1]);
+}
+
+// One round of V bits at a compile-time offset B on every group of the thread.
+template <int K, int C, bool DIF, bool INV, int B, int V, int Q = 0>
+__device__ __forceinline__ void compute_groups(uint64_t (&x)[16], const uint64_t *pw, uint32_t tid,
+                                               uint32_t nthreads) {
+  constexpr int NV = 1 << V, NG = 16 / NV;
+  if constexpr (Q < NG) {
+    uint32_t w;
+    group_base<K, C, B, V>(tid + nthreads * Q, w);
+    const uint64_t *pp = pw + ((1u << (K - B - V)) - 1) + (NV - 1) * (w >> (B + V));
+    if constexpr (!DIF) mul_powers<V, Q * NV>(x, pp);
+    cnet<DIF, INV, V, Q * NV>(x);
+    if constexpr (DIF) mul_powers<V, Q * NV>(x, pp);
+    compute_groups<K, C, DIF, INV, B, V, Q + 1>(x, pw, tid, nthreads);
+  }
+}
+
 // Rounds [RI, END) through shared memory, each followed by a barrier
-// (END = -1: through the last round).
-template <int K, int C, bool DIF, bool RAGGED_FIRST, int RI, int END = -1>
-__device__ __forceinline__ void rounds_from(uint64_t *tile, const uint64_t *tws, uint32_t tid, uint32_t nthreads) {
+// (END = -1: through the last round).  DIF rounds run short-round-first, the
+// partition the power table is laid out for.
+template <int K, int C, bool DIF, bool INV, bool RAGGED_FIRST, int RI, int END = -1>
+__device__ __forceinline__ void rounds_from(uint64_t *tile, const uint64_t *pw, uint32_t tid, uint32_t nthreads) {
+  static_assert(!DIF || RAGGED_FIRST || K % 4 == 0 || K < 4, "DIF rounds must take the short round first");
   using S = RoundShape<K, DIF, RAGGED_FIRST, RI>;
   constexpr int STOP = END < 0 ? S::NR : END;
   if constexpr (RI < STOP) {
     uint64_t x[16];
     load_groups<K, C, S::B, S::V>(tile, x, tid, nthreads);
-    compute_groups<K, C, DIF, S::B, S::V>(x, tws, tid, nthreads);
+    compute_groups<K, C, DIF, INV, S::B, S::V>(x, pw, tid, nthreads);
     store_groups<K, C, S::B, S::V>(tile, x, tid, nthreads);
     __syncthreads();
-    rounds_from<K, C, DIF, RAGGED_FIRST, RI + 1, END>(tile, tws, tid, nthreads);
-  }
-}
-
-// Shared-memory twiddles of one tile position: entry 2^(K-1-q) + u holds
-// T[(H << (K-1-q)) + u], q = window bit.
-template <int K>
-__device__ __forceinline__ void fill_twiddles(uint64_t *tws, const DevTables &tabs, uint32_t inv, uint32_t H,
-                                              uint32_t tid, uint32_t nthreads) {
-  for (uint32_t t = tid + 1; t < (1u << K); t += nthreads) {
-    const uint32_t level = 31 - __clz(t); // = K - 1 - (window bit)
-    const uint32_t u = t - (1u << level);
-    tws[tw_slot(t)] = twiddle(tabs, inv, (H << level) + u);
+    rounds_from<K, C, DIF, INV, RAGGED_FIRST, RI + 1, END>(tile, pw, tid, nthreads);
   }
 }
 
@@ -256,7 +335,7 @@ __device__ __forceinline__ void fill_twiddles(uint64_t *tws, const DevTables &ta
 // A full round holds 4 window bits [B, B + 4) of one group per thread.  The
 // network below is written once per direction and reused for every full
 // round of a pass (looped with `#pragma unroll 1`), which keeps a kernel to one
-// copy of the 32-butterfly register network instead of one per round.
+// copy of the register network instead of one per round.
 
 // Tile index of element 0 of group gi (runs of C fastest) and its window value w.
 template <int K, int C>
@@ -282,38 +361,21 @@ __device__ __forceinline__ void slots16(uint32_t eb, uint32_t S, uint32_t (&a)[1
   }
 }
 
-// The four stages of a full round on x[16] (element j at window w | j << B).
-// The twiddle of stage bit qb for element pair j0 is entry
-// 2^(K-1-qb) + (w >> (qb+1)) + (j0 >> (qq+1)) of the tile's table; the last
-// term never carries across a pad word, so one base pointer per stage serves
-// all its pairs with constant offsets.
-template <int K, bool DIF>
-__device__ __forceinline__ void net16(uint64_t (&x)[16], const uint64_t *tws, uint32_t w, uint32_t B) {
-  const uint64_t *tp[4];
-#pragma unroll
-  for (int qq = 0; qq < 4; qq++) {
-    const uint32_t qb = B + qq;
-    tp[qq] = tws + tw_slot((1u << (K - 1 - qb)) + (w >> (qb + 1)));
-  }
-#pragma unroll
-  for (int st = 0; st < 4; st++) {
-    const int qq = DIF ? st : 3 - st;
-#pragma unroll
-    for (int j0 = 0; j0 < 16; j0++) {
-      if (j0 & (1 << qq)) continue;
-      const uint64_t t = tp[qq][j0 >> (qq + 1)];
-      if (DIF)
-        dif(x[j0], x[j0 | (1 << qq)], t);
-      else
-        dit(x[j0], x[j0 | (1 << qq)], t);
-    }
-  }
+// A full round on x[16] (element j at window w | j << B).  scale = false skips
+// the multiplications by s^j, for a caller that knows s = 1 (R = 0) or has
+// folded s^j into its own scaling.
+template <int K, bool DIF, bool INV>
+__device__ __forceinline__ void net16(uint64_t (&x)[16], const uint64_t *pw, uint32_t w, uint32_t B, bool scale) {
+  const uint64_t *pp = pw + ((1u << (K - 4 - B)) - 1) + 15 * (w >> (B + 4));
+  if (!DIF && scale) mul_powers<4, 0>(x, pp);
+  cnet<DIF, INV, 4, 0>(x);
+  if (DIF && scale) mul_powers<4, 0>(x, pp);
 }
 
 // Full rounds at bit offsets B0, B0 + dB, ... (count rounds) through shared
 // memory, each followed by a barrier.  One thread per group.
-template <int K, int C, bool DIF>
-__device__ __forceinline__ void full_rounds(uint64_t *tile, const uint64_t *tws, int B0, int dB, int count,
+template <int K, int C, bool DIF, bool INV>
+__device__ __forceinline__ void full_rounds(uint64_t *tile, const uint64_t *pw, int B0, int dB, int count,
                                             uint32_t tid) {
 #pragma unroll 1
   for (int r = 0; r < count; r++) {
@@ -325,7 +387,7 @@ __device__ __forceinline__ void full_rounds(uint64_t *tile, const uint64_t *tws,
     uint64_t x[16];
 #pragma unroll
     for (int j = 0; j < 16; j++) x[j] = tile[a[j]];
-    net16<K, DIF>(x, tws, w, B);
+    net16<K, DIF, INV>(x, pw, w, B, true);
 #pragma unroll
     for (int j = 0; j < 16; j++) tile[a[j]] = x[j];
     __syncthreads();
@@ -381,7 +443,13 @@ __device__ __forceinline__ void tile_elem(uint32_t e, uint32_t &g, uint64_t &off
 // the tile is loaded with 16-byte loads, the short round runs first at the
 // bottom, the full rounds upwards, and the last full round (top 4 bits) is
 // stored straight from registers.
-template <int K, int C, bool B2N>
+//
+// Twiddles.  INV selects the inverse table (p.inverse); the power table of the
+// tile position sits after the tile.  The window's top round has R = H: for
+// H = 0 its s is 1 and its multiplications are skipped, and where the pass
+// scales on load (n2b) or on store (b2n) the top round's s^j is folded into
+// that scaling's running product.
+template <int K, int C, bool B2N, bool INV>
 __device__ __forceinline__ void pass_body(const PassParams &p, uint32_t bx, uint32_t by, uint64_t *smem) {
   constexpr int W = 1 << K;
   constexpr int R = K % 4, NF = K / 4;
@@ -389,11 +457,12 @@ __device__ __forceinline__ void pass_body(const PassParams &p, uint32_t bx, uint
   const uint32_t TILE = G * W * C;
   const uint32_t T = TILE / 16; // == blockDim.x
   uint64_t *tile = smem;
-  uint64_t *tws = smem + TILE + TILE / 16;
+  uint64_t *pw = smem + TILE + TILE / 16;
   const uint32_t tid = threadIdx.x;
   const TileGeom tg = tile_geom<K, C>(p, bx, by);
   const uint32_t Hbig = tg.H + (brev_bits(tg.group, p.log_groups) << (p.log_n - p.lb - K));
-  fill_twiddles<K>(tws, p.tabs, p.inverse, Hbig, tid, T);
+  fill_powers<K>(pw, p.tabs, INV, Hbig, tid, T);
+  const bool top_s = Hbig != 0; // the top round's s differs from 1
 
   const uint64_t *in = p.in + tg.group * p.group_stride_in;
   uint64_t *out = p.out + tg.group * p.group_stride_out;
@@ -408,7 +477,7 @@ __device__ __forceinline__ void pass_body(const PassParams &p, uint32_t bx, uint
 
   for (uint32_t c0 = tg.col_begin; c0 < tg.col_end; c0 += G) {
     if constexpr (!B2N && NF > 0) {
-      __syncthreads(); // twiddles ready; previous column group's stores done
+      __syncthreads(); // powers ready; previous column group's stores done
       // first full round straight from global memory
       constexpr uint32_t B = K - 4;
       uint32_t w;
@@ -422,8 +491,9 @@ __device__ __forceinline__ void pass_body(const PassParams &p, uint32_t bx, uint
         const uint64_t step = 1ull << (B + p.lb);
 #pragma unroll
         for (int j = 0; j < 16; j++) x[j] = __ldcg(src + j * step);
-        if (p.load_scale) { // c^i for i = off0 + j * step: a running product
-          const uint64_t c_step = coset_power(p.tabs, 0, (uint32_t)step, p.coset_kshift);
+        if (p.load_scale) { // c^i s^j for i = off0 + j * step: a running product
+          uint64_t c_step = coset_power(p.tabs, 0, (uint32_t)step, p.coset_kshift);
+          if (top_s) c_step = gl::mul(c_step, pw[0]);
           uint64_t c = coset_power(p.tabs, 0, (uint32_t)off0, p.coset_kshift);
 #pragma unroll
           for (int j = 0; j < 16; j++) {
@@ -435,14 +505,14 @@ __device__ __forceinline__ void pass_body(const PassParams &p, uint32_t bx, uint
 #pragma unroll
         for (int j = 0; j < 16; j++) x[j] = 0;
       }
-      net16<K, false>(x, tws, w, B);
+      net16<K, false, INV>(x, pw, w, B, top_s && !p.load_scale);
       uint32_t a[16];
       slots16(eb, (uint32_t)C << B, a);
 #pragma unroll
       for (int j = 0; j < 16; j++) tile[a[j]] = x[j];
       __syncthreads();
-      full_rounds<K, C, false>(tile, tws, (int)B - 4, -4, NF - 1, tid);
-      if constexpr (R > 0) rounds_from<K, C, false, false, NF>(tile, tws, tid, T);
+      full_rounds<K, C, false, INV>(tile, pw, (int)B - 4, -4, NF - 1, tid);
+      if constexpr (R > 0) rounds_from<K, C, false, INV, false, NF>(tile, pw, tid, T);
     } else {
 #pragma unroll
       for (int j = 0; j < 8; j++) {
@@ -475,12 +545,12 @@ __device__ __forceinline__ void pass_body(const PassParams &p, uint32_t bx, uint
       }
       __syncthreads();
       if constexpr (!B2N) {
-        rounds_from<K, C, false, false, 0>(tile, tws, tid, T); // K < 4: one short round
+        rounds_from<K, C, false, INV, false, 0>(tile, pw, tid, T); // K < 4: one short round
       } else if constexpr (NF == 0) {
-        rounds_from<K, C, true, true, 0>(tile, tws, tid, T);
+        rounds_from<K, C, true, INV, true, 0>(tile, pw, tid, T);
       } else {
-        if constexpr (R > 0) rounds_from<K, C, true, true, 0, 1>(tile, tws, tid, T);
-        full_rounds<K, C, true>(tile, tws, R, 4, NF - 1, tid);
+        if constexpr (R > 0) rounds_from<K, C, true, INV, true, 0, 1>(tile, pw, tid, T);
+        full_rounds<K, C, true, INV>(tile, pw, R, 4, NF - 1, tid);
         // last full round (top 4 bits) stored straight from registers
         constexpr uint32_t B = K - 4;
         uint32_t w;
@@ -490,19 +560,20 @@ __device__ __forceinline__ void pass_body(const PassParams &p, uint32_t bx, uint
         uint64_t x[16];
 #pragma unroll
         for (int j = 0; j < 16; j++) x[j] = tile[a[j]];
-        net16<K, true>(x, tws, w, B);
+        net16<K, true, INV>(x, pw, w, B, top_s && !p.store_scale);
         uint64_t off0;
         uint32_t col;
         group_origin(eb, c0, off0, col);
         if (col < tg.col_end) {
           uint64_t *dst = out + (uint64_t)col * p.stride_out + off0;
           const uint64_t step = 1ull << (B + p.lb);
-          if (p.store_scale) { // n^-1 c^-i for the natural index i = off0 + j * step: a running product
+          if (p.store_scale) { // n^-1 c^-i s^j for the natural index i = off0 + j * step: a running product
             uint64_t s = p.tabs.inv_pow2[p.log_n], s_step = 1;
             if (p.has_coset) {
               s = gl::mul(s, coset_power(p.tabs, 1, (uint32_t)off0, p.coset_kshift));
               s_step = coset_power(p.tabs, 1, (uint32_t)step, p.coset_kshift);
             }
+            if (top_s) s_step = p.has_coset ? gl::mul(s_step, pw[0]) : pw[0];
 #pragma unroll
             for (int j = 0; j < 16; j++) {
               x[j] = gl::mul(x[j], s);
@@ -556,14 +627,15 @@ __device__ __forceinline__ void pass_body(const PassParams &p, uint32_t bx, uint
 }
 
 // Shared memory (u64 words) of pass_body for a tile of `tile` elements.
-__host__ __device__ constexpr uint32_t pass_smem_words(uint32_t tile, int K) {
-  return tile + tile / 16 + (1u << K) + (1u << K) / 16;
-}
+__host__ __device__ constexpr uint32_t pass_smem_words(uint32_t tile, int K) { return tile + tile / 16 + (1u << K); }
 
 template <int K, int C, bool B2N>
 __global__ void __launch_bounds__(256, BC_PASS_MIN_BLOCKS) ntt_pass_kernel(const PassParams p) {
   extern __shared__ uint64_t smem[];
-  pass_body<K, C, B2N>(p, blockIdx.x, blockIdx.y, smem);
+  if (p.inverse)
+    pass_body<K, C, B2N, true>(p, blockIdx.x, blockIdx.y, smem);
+  else
+    pass_body<K, C, B2N, false>(p, blockIdx.x, blockIdx.y, smem);
 }
 
 } // namespace bc

@@ -34,6 +34,15 @@ constexpr int PW_LOG = 30;   // LDE domains up to 2^30 (log_n + log_blowup <= 30
 constexpr int PW_FINE = 15;  // w_lo: 2^15, w_hi: 2^15
 constexpr int MAX_LOG_N = TW_LOG;
 
+// The first eight twiddles are signed powers of two.  T[u] = w_16^{brev_3(u)}
+// for u < 8, and w_16 = w_{2^32}^{2^28} = 2^156 (mod p), so T[u] = 2^e with e
+// below (mod 192; 2^96 = -1, so e >= 96 is -2^(e-96)).  Inverse: 2^(192 - e).
+// The context checks these against its tables when it is created.
+__host__ __device__ constexpr int small_tw_exp(bool inv, int u) {
+  constexpr int fwd[8] = {0, 48, 120, 168, 156, 12, 84, 132};
+  return inv ? (192 - fwd[u]) % 192 : fwd[u];
+}
+
 struct DevTables {
   const uint64_t *tw_lo[2]; // [0] forward, [1] inverse
   const uint64_t *tw_hi[2];
