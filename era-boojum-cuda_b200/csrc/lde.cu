@@ -31,7 +31,7 @@
 namespace bc {
 
 template <int K, int C>
-__global__ void __launch_bounds__(256, 2) lde_top_kernel(const LdeTopParams p) {
+__global__ void __launch_bounds__(256, BC_TOP_MIN_BLOCKS) lde_top_kernel(const LdeTopParams p) {
   extern __shared__ uint64_t smem[];
   top_body<K, C>(p, blockIdx.x, blockIdx.y, smem);
 }

@@ -42,10 +42,20 @@
 #include "gl.cuh"
 #include "tables.cuh"
 
-// Resident CTAs per SM the pass kernels are compiled for (256 threads each);
-// 2 leaves each thread 128 registers, enough for 16 values without spills.
+// Resident CTAs per SM the pass kernels are compiled for (256 threads each):
+// natural->bit-reversed passes 2 (128 registers a thread), bit-reversed->natural
+// ones 3 (80 registers; measured ~9 % faster on B200, while the n2b ones gain
+// nothing from the third CTA) except the windows of fewer than 9 bits with
+// runs of 8, which spill at 80 registers.
 #ifndef BC_PASS_MIN_BLOCKS
 #define BC_PASS_MIN_BLOCKS 2
+#endif
+#ifndef BC_PASS_MIN_BLOCKS_B2N
+#define BC_PASS_MIN_BLOCKS_B2N 3
+#endif
+// The same for the fused LDE's top-window kernel (lde.cu).
+#ifndef BC_TOP_MIN_BLOCKS
+#define BC_TOP_MIN_BLOCKS 2
 #endif
 
 namespace bc {
@@ -630,7 +640,8 @@ __device__ __forceinline__ void pass_body(const PassParams &p, uint32_t bx, uint
 __host__ __device__ constexpr uint32_t pass_smem_words(uint32_t tile, int K) { return tile + tile / 16 + (1u << K); }
 
 template <int K, int C, bool B2N>
-__global__ void __launch_bounds__(256, BC_PASS_MIN_BLOCKS) ntt_pass_kernel(const PassParams p) {
+__global__ void __launch_bounds__(256, (B2N && (K >= 9 || C == 1)) ? BC_PASS_MIN_BLOCKS_B2N : BC_PASS_MIN_BLOCKS)
+    ntt_pass_kernel(const PassParams p) {
   extern __shared__ uint64_t smem[];
   if (p.inverse)
     pass_body<K, C, B2N, true>(p, blockIdx.x, blockIdx.y, smem);
