@@ -361,6 +361,8 @@ def run_ours(args, rank, world):
         line["large"] = run_large_section()
     if world == 1 and not args.no_serve:
         line["serve"] = run_serve_section()
+    if world == 1 and not args.no_ops:
+        line["ops"] = run_ops_section(ops_ours())
     return line
 
 
@@ -512,6 +514,86 @@ def run_large_section(reps: int = 5):
             "plain_hbm_frac": round(alg / (t_p / 1e3) / 1e9 / peak, 4), "bit_exact_fused_vs_plain": exact}
 
 
+def run_ops_section(ops, reps: int = 5):
+    """The ops beside the NTT (include/bc_ops.h; src/ops_complex.rs) on HBM-sized inputs.
+
+    `ops` maps an op name to a callable (src_ptr, dst_ptr, stream) -> None: this library's entry points in the
+    ours arm, the reference's own kernels in the reference arm, on the same workloads.  Every op is bound by
+    HBM traffic: 16 bytes per element for the bit reversal and the omega shift (read + write), 8 for the
+    powers (write only); achieved = those bytes / event-timed duration, frac of the measured copy peak.
+    """
+    import torch
+
+    peak, peak_kind = measured_peaks()
+    n_vec = 1 << 28                       # 2 GiB of u64, larger than L2
+    log_rows, cols = 22, 64               # bit reversal: 64 columns x 2^22 rows = 2 GiB
+    a = torch.randint(-(2**63), 2**63 - 1, (n_vec,), device="cuda", dtype=torch.int64,
+                      generator=torch.Generator(device="cuda").manual_seed(5))
+    b = torch.empty_like(a)
+    stream = torch.cuda.current_stream()
+    work = {  # name -> (elements, bytes per element, workload)
+        "bit_reverse": (cols << log_rows, 16, f"{cols} cols x 2^{log_rows}, out of place"),
+        "bit_reverse_in_place": (cols << log_rows, 16, f"{cols} cols x 2^{log_rows}, in place"),
+        "omega_shift": (n_vec, 16, "2^28 elements, log_degree 24, shift 3"),
+        "get_powers_of_w": (n_vec, 8, "2^28 elements, log_degree 24"),
+        "get_powers_of_g": (n_vec, 8, "2^28 elements, log_degree 24"),
+        "get_powers_by_val_bf": (n_vec, 8, "2^28 elements, base 42"),
+    }
+    res = {}
+    for name, fn in ops.items():
+        elems, bpe, workload = work[name]
+        fn(a.data_ptr(), b.data_ptr(), stream.cuda_stream)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn(a.data_ptr(), b.data_ptr(), stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        gbs = elems * bpe / (ms / 1e3) / 1e9
+        res[name] = {"workload": workload, "ms": round(ms, 4), "gelem_per_s": round(elems / (ms / 1e3) / 1e9, 2),
+                     "achieved_gbs": round(gbs, 1), "hbm_frac": round(gbs / peak, 4)}
+    del a, b
+    torch.cuda.empty_cache()
+    res["peak_gbs"] = peak
+    res["peak_kind"] = peak_kind
+    return res
+
+
+def ops_ours():
+    """This library's ops, as run_ops_section callables."""
+    import bc_ntt
+
+    L = bc_ntt.lib()
+    rows, cols, n = 1 << 22, 64, 1 << 28
+
+    def ck(rc):
+        assert rc == 0, rc
+
+    return {
+        "bit_reverse": lambda a, b, s: ck(L.bc_bit_reverse(a, rows, b, rows, 22, cols, s)),
+        "bit_reverse_in_place": lambda a, b, s: ck(L.bc_bit_reverse_in_place(a, rows, 22, cols, s)),
+        "omega_shift": lambda a, b, s: ck(L.bc_omega_shift(a, 24, 0, False, 3, b, n, s)),
+        "get_powers_of_w": lambda a, b, s: ck(L.bc_get_powers_of_w(24, 0, False, False, b, n, s)),
+        "get_powers_of_g": lambda a, b, s: ck(L.bc_get_powers_of_g(24, 0, False, False, b, n, s)),
+        "get_powers_by_val_bf": lambda a, b, s: ck(L.bc_get_powers_by_val_bf(42, 0, False, b, n, s)),
+    }
+
+
+def ops_reference(ref):
+    """The reference's own ops kernels (oracle.RefKernels), as run_ops_section callables."""
+    rows, cols, n = 1 << 22, 64, 1 << 28
+    return {
+        "bit_reverse": lambda a, b, s: ref.bit_reverse(a, rows, b, rows, 22, cols, s),
+        "bit_reverse_in_place": lambda a, b, s: ref.bit_reverse(a, rows, a, rows, 22, cols, s),
+        "omega_shift": lambda a, b, s: ref.omega_shift(a, 24, 0, False, 3, b, n, s),
+        "get_powers_of_w": lambda a, b, s: ref.get_powers_of(24, 0, False, False, False, b, n, s),
+        "get_powers_of_g": lambda a, b, s: ref.get_powers_of(24, 0, False, False, True, b, n, s),
+        "get_powers_by_val_bf": lambda a, b, s: ref.get_powers_by_val(42, 0, False, b, n, s),
+    }
+
+
 def run_serve_section(n_requests: int = 48, rate: float = 20.0, budget_gib: int = 40, slots: int = 4):
     """Poisson LDE requests through the continuous-batching server vs the same requests served one at a time.
 
@@ -627,7 +709,10 @@ def run_reference(args, rank, world):
 
     e2e_steps = max(2, min(args.steps, 5))
     e2e_ms, _ = time_steps(e2e_step, e2e_steps, 1, world, stream)
-    return {
+    del dx, hx, hout, x, out, coef
+    torch.cuda.empty_cache()
+    ops = run_ops_section(ops_reference(ref)) if world == 1 and not args.no_ops else None
+    line = {
         "metric": METRIC, "value": round(value, 1), "unit": "Melem/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u64 (Goldilocks)", "data": "synthetic", "impl": "reference",
@@ -642,6 +727,9 @@ def run_reference(args, rank, world):
                 "h2d_bytes_per_step": 8 * COLS * n, "d2h_bytes_per_step": 8 * B * COLS * n,
                 "ms_per_step": round(e2e_ms / e2e_steps, 3)},
     }
+    if ops is not None:
+        line["ops"] = ops
+    return line
 
 
 def main():
@@ -654,6 +742,7 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the uneven-batch section")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving section")
     ap.add_argument("--no-large", action="store_true", help="skip the 64 x 2^23 blowup-4 section")
+    ap.add_argument("--no-ops", action="store_true", help="skip the bit-reversal / powers / omega-shift section")
     ap.add_argument("--no-tuned-plans", action="store_true", help="ignore the autotuned plan file")
     ap.add_argument("--log-n", type=int, default=22, help="column length 2^log_n (default 22)")
     ap.add_argument("--cols", type=int, default=128, help="columns (default 128)")

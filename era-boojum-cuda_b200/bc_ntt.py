@@ -4,7 +4,9 @@ The reference exposes ``boojum_cuda::ntt::{batch_ntt_internal,
 batch_ntt_out_of_place, batch_ntt_in_place}`` (src/ntt.rs:179-369) and
 ``boojum_cuda::context::Context::{create, destroy}`` (src/context.rs:171-296).
 This module exposes the same operations, with the same argument meaning, over
-the C ABI declared in include/bc_ntt.h.  Device buffers are torch CUDA tensors
+the C ABI declared in include/bc_ntt.h, and the ops of src/ops_complex.rs
+(bit_reverse, get_powers_of_w/g, get_powers_by_val/ref, omega_shift) over
+include/bc_ops.h.  Device buffers are torch CUDA tensors
 of dtype int64 or uint64 (the words are reinterpreted, never converted);
 streams default to torch's current stream.
 
@@ -70,6 +72,16 @@ SIGNATURES = {
     "bc_lde_server_cancel": [_vp, _u64],
     "bc_lde_server_get_stats": [_vp, _vp],
     "bc_lde_server_destroy": [_vp],
+    "bc_bit_reverse": [_vp, _u64, _vp, _u64, _u32, _u32, _vp],
+    "bc_bit_reverse_in_place": [_vp, _u64, _u32, _u32, _vp],
+    "bc_get_powers_of_w": [_u32, _u32, _b, _b, _vp, _u32, _vp],
+    "bc_get_powers_of_g": [_u32, _u32, _b, _b, _vp, _u32, _vp],
+    "bc_get_powers_by_val_bf": [_u64, _u32, _b, _vp, _u32, _vp],
+    "bc_get_powers_by_ref_bf": [_vp, _u32, _b, _vp, _u32, _vp],
+    "bc_get_powers_by_val_ef": [_u64, _u64, _u32, _b, _vp, _u32, _vp],
+    "bc_get_powers_by_ref_ef": [_vp, _u32, _b, _vp, _u32, _vp],
+    "bc_omega_shift": [_vp, _u32, _u32, _b, _u32, _vp, _u32, _vp],
+    "bc_omega_shift_in_place": [_vp, _u32, _u32, _b, _u32, _u32, _vp],
 }
 
 CUDA_ERROR_NOT_READY = 600
@@ -346,3 +358,88 @@ def load_tuned_plans(path: str = PLANS_PATH) -> bool:
     text = "".join(line for line in open(path) if line.strip() and not line.startswith("#"))
     plan_table_import(text)
     return True
+
+
+# ---------------------------------------------------------------- ops (src/ops_complex.rs, include/bc_ops.h)
+def _u32_count(n: int, what: str) -> int:
+    if n > 0xFFFFFFFF:
+        raise ValueError(f"{what}: more than 2^32 - 1 elements")
+    return n
+
+
+def bit_reverse(src, dst, log_rows: int, cols: int, src_stride: int | None = None, dst_stride: int | None = None,
+                stream=None):
+    """bit_reverse (src/ops_complex.rs:306-318): dst[brev(i)] = src[i] in each column of 2^log_rows rows."""
+    rows = 1 << log_rows
+    ss = rows if src_stride is None else src_stride
+    ds = rows if dst_stride is None else dst_stride
+    if cols and (_len(src) < (cols - 1) * ss + rows or _len(dst) < (cols - 1) * ds + rows):
+        raise ValueError("bit_reverse: matrix does not fit its buffer")
+    _check(lib().bc_bit_reverse(_ptr(src), ss, _ptr(dst), ds, log_rows, cols, _stream(stream)), "bit_reverse")
+
+
+def bit_reverse_in_place(values, log_rows: int, cols: int, stride: int | None = None, stream=None):
+    """bit_reverse_in_place (src/ops_complex.rs:320-329)."""
+    rows = 1 << log_rows
+    st = rows if stride is None else stride
+    if cols and _len(values) < (cols - 1) * st + rows:
+        raise ValueError("bit_reverse_in_place: matrix does not fit its buffer")
+    _check(lib().bc_bit_reverse_in_place(_ptr(values), st, log_rows, cols, _stream(stream)), "bit_reverse_in_place")
+
+
+def get_powers_of_w(log_degree: int, offset: int, inverse: bool, bit_reverse: bool, result, stream=None):
+    """get_powers_of_w (src/ops_complex.rs:40-85): len(result) powers of w_{2^log_degree}."""
+    n = _u32_count(_len(result), "get_powers_of_w")
+    _check(lib().bc_get_powers_of_w(log_degree, offset, inverse, bit_reverse, _ptr(result), n, _stream(stream)),
+           "get_powers_of_w")
+
+
+def get_powers_of_g(log_degree: int, offset: int, inverse: bool, bit_reverse: bool, result, stream=None):
+    """get_powers_of_g (src/ops_complex.rs:40-86): len(result) powers of 7^(2^(24 - log_degree))."""
+    n = _u32_count(_len(result), "get_powers_of_g")
+    _check(lib().bc_get_powers_of_g(log_degree, offset, inverse, bit_reverse, _ptr(result), n, _stream(stream)),
+           "get_powers_of_g")
+
+
+def get_powers_by_val(base, offset: int, bit_reverse: bool, result, stream=None):
+    """get_powers_by_val (src/ops_complex.rs:117-131).  base: int (base field; len(result) powers) or
+    (c0, c1) (extension; result holds 2 * count words, all c0 then all c1)."""
+    if isinstance(base, (tuple, list)):
+        n = _u32_count(_len(result) // 2, "get_powers_by_val")
+        _check(lib().bc_get_powers_by_val_ef(base[0], base[1], offset, bit_reverse, _ptr(result), n,
+                                             _stream(stream)), "get_powers_by_val")
+    else:
+        n = _u32_count(_len(result), "get_powers_by_val")
+        _check(lib().bc_get_powers_by_val_bf(base, offset, bit_reverse, _ptr(result), n, _stream(stream)),
+               "get_powers_by_val")
+
+
+def get_powers_by_ref(base, offset: int, bit_reverse: bool, result, ext: bool = False, stream=None):
+    """get_powers_by_ref (src/ops_complex.rs:176-190): base is a device tensor holding the base (1 word, or
+    2 words for the extension)."""
+    if ext:
+        if _len(base) < 2:
+            raise ValueError("get_powers_by_ref: an extension base takes 2 words")
+        n = _u32_count(_len(result) // 2, "get_powers_by_ref")
+        _check(lib().bc_get_powers_by_ref_ef(_ptr(base), offset, bit_reverse, _ptr(result), n, _stream(stream)),
+               "get_powers_by_ref")
+    else:
+        n = _u32_count(_len(result), "get_powers_by_ref")
+        _check(lib().bc_get_powers_by_ref_bf(_ptr(base), offset, bit_reverse, _ptr(result), n, _stream(stream)),
+               "get_powers_by_ref")
+
+
+def omega_shift(src, log_degree: int, offset: int, inverse: bool, shift: int, dst, stream=None):
+    """omega_shift (src/ops_complex.rs:226-242): dst[i] = src[i] * w^(shift * (i + offset)), w = w_{2^log_degree}."""
+    if _len(src) != _len(dst):
+        raise ValueError("omega_shift: src and dst lengths differ")
+    n = _u32_count(_len(dst), "omega_shift")
+    _check(lib().bc_omega_shift(_ptr(src), log_degree, offset, inverse, shift, _ptr(dst), n, _stream(stream)),
+           "omega_shift")
+
+
+def omega_shift_in_place(values, log_degree: int, offset: int, inverse: bool, shift: int, stream=None):
+    """omega_shift_in_place (src/ops_complex.rs:244-258)."""
+    n = _u32_count(_len(values), "omega_shift_in_place")
+    _check(lib().bc_omega_shift_in_place(_ptr(values), log_degree, offset, inverse, shift, n, _stream(stream)),
+           "omega_shift_in_place")

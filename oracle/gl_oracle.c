@@ -262,3 +262,87 @@ void gl_oracle_dft_naive(const uint64_t *x, uint64_t *y, unsigned log_n, int inv
 void gl_oracle_canonicalize(uint64_t *x, uint64_t count) {
   for (uint64_t i = 0; i < count; i++) x[i] = gl_canon(x[i]);
 }
+
+/* ------------------------------------------------------------------ ops beside the NTT
+ * Restatements of the reference's src/ops_complex.rs operations with the
+ * index conventions of its kernels (native/ops_complex.cu:9-157) and of its
+ * power tables (native/context.cuh:9-48: omega = w_{2^24}, exponents mod
+ * 2^24, inverse = w^-e; g = 7).  Element by element, with full
+ * exponentiations, so they share nothing with the product's tables or running
+ * products. */
+
+static inline uint32_t brev32(uint32_t x) { return brev(x, 32); }
+
+/* dst[brev_{log_rows}(i)] = src[i] in each column (src and dst distinct). */
+void gl_oracle_bit_reverse(const uint64_t *src, uint64_t src_stride, uint64_t *dst, uint64_t dst_stride,
+                           unsigned log_rows, uint32_t cols) {
+  const uint64_t rows = 1ull << log_rows;
+  for (uint32_t c = 0; c < cols; c++)
+    for (uint64_t i = 0; i < rows; i++) dst[c * dst_stride + brev((uint32_t)i, log_rows)] = src[c * src_stride + i];
+}
+
+/* native/ops_complex.cu:9-33: r = i + offset (u32), idx = bit_reverse ?
+ * brev_{log_degree}(r) : r, e = (idx << (24 - log_degree)) mod 2^24; the
+ * value is w_{2^24}^e (of_g = 0) or 7^e (of_g = 1), inverted bases when
+ * inverse. */
+void gl_oracle_powers_of(unsigned log_degree, uint32_t offset, int inverse, int bit_reverse, int of_g,
+                         uint64_t *result, uint32_t count) {
+  uint64_t base = of_g ? 7 : gl_oracle_root_of_unity(24);
+  if (inverse) base = gl_oracle_inv(base);
+  for (uint32_t i = 0; i < count; i++) {
+    const uint32_t r = i + offset;
+    const uint32_t idx = bit_reverse ? brev(r & (log_degree ? (uint32_t)((1ull << log_degree) - 1) : 0u), log_degree) : r;
+    const uint32_t e = (uint32_t)(idx << (24 - log_degree)) & ((1u << 24) - 1);
+    result[i] = gl_oracle_pow(base, e);
+  }
+}
+
+/* Quadratic extension F_p[x] / (x^2 - 7) (native/goldilocks_extension.cuh:11-80). */
+static void ext_mul(const uint64_t a[2], const uint64_t b[2], uint64_t r[2]) {
+  const uint64_t c0 = gl_add(gl_mul(a[0], b[0]), gl_mul(7, gl_mul(a[1], b[1])));
+  const uint64_t c1 = gl_add(gl_mul(a[0], b[1]), gl_mul(a[1], b[0]));
+  r[0] = c0;
+  r[1] = c1;
+}
+
+static void ext_pow(const uint64_t base[2], uint32_t e, uint64_t r[2]) {
+  uint64_t acc[2] = {1, 0}, b[2] = {gl_canon(base[0]), gl_canon(base[1])};
+  while (e) {
+    if (e & 1) ext_mul(acc, b, acc);
+    ext_mul(b, b, b);
+    e >>= 1;
+  }
+  r[0] = acc[0];
+  r[1] = acc[1];
+}
+
+/* native/ops_complex.cu:35-74: e = (bit_reverse ? brev_32(i) : i) + offset
+ * (u32), result[i] = base^e; the extension version stores its two
+ * coordinates at result[i] and result[i + count]. */
+void gl_oracle_powers_by(uint64_t base_c0, uint64_t base_c1, int ext, uint32_t offset, int bit_reverse,
+                         uint64_t *result, uint32_t count) {
+  const uint64_t base[2] = {base_c0, base_c1};
+  for (uint32_t i = 0; i < count; i++) {
+    const uint32_t e = (bit_reverse ? brev32(i) : i) + offset;
+    if (ext) {
+      uint64_t v[2];
+      ext_pow(base, e, v);
+      result[i] = v[0];
+      result[(uint64_t)count + i] = v[1];
+    } else {
+      result[i] = gl_oracle_pow(base_c0, e);
+    }
+  }
+}
+
+/* native/ops_complex.cu:76-87: dst[i] = src[i] * w_{2^24}^{+-e},
+ * e = ((shift * (i + offset)) << (24 - log_degree)) mod 2^24 in u32 arithmetic. */
+void gl_oracle_omega_shift(const uint64_t *src, unsigned log_degree, uint32_t offset, int inverse, uint32_t shift,
+                           uint64_t *dst, uint32_t count) {
+  uint64_t w = gl_oracle_root_of_unity(24);
+  if (inverse) w = gl_oracle_inv(w);
+  for (uint32_t i = 0; i < count; i++) {
+    const uint32_t e = (uint32_t)((shift * (i + offset)) << (24 - log_degree)) & ((1u << 24) - 1);
+    dst[i] = gl_mul(gl_canon(src[i]), gl_oracle_pow(w, e));
+  }
+}

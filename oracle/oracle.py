@@ -5,8 +5,10 @@ cpu_baseline / reference legs of bench.py -- never by the product library.
 
 * ``batch_ntt`` / ``lde``: CPU restatement (gl_oracle.c) of src/ntt.rs:179-369
   semantics, numpy uint64 arrays in and out.
+* ``bit_reverse`` / ``powers_of`` / ``powers_by`` / ``omega_shift``: CPU
+  restatements (gl_oracle.c) of the ops in src/ops_complex.rs.
 * ``RefKernels``: the reference's own CUDA kernels (native/ntt.cu,
-  native/context.cu) built into oracle/_ref/libref_ntt.so by
+  native/context.cu, native/ops_complex.cu) built into oracle/_ref/libref_ntt.so by
   ``make -C oracle ref``, driven by ref_glue.cu's restatement of
   Context::create and batch_ntt_internal.
 """
@@ -45,6 +47,14 @@ def lib():
         L.gl_oracle_mul.restype = _u64
         L.gl_oracle_pow.argtypes = [_u64, _u64]
         L.gl_oracle_pow.restype = _u64
+        L.gl_oracle_bit_reverse.argtypes = [_vp, _u64, _vp, _u64, _u32, _u32]
+        L.gl_oracle_bit_reverse.restype = None
+        L.gl_oracle_powers_of.argtypes = [_u32, _u32, _i32, _i32, _i32, _vp, _u32]
+        L.gl_oracle_powers_of.restype = None
+        L.gl_oracle_powers_by.argtypes = [_u64, _u64, _i32, _u32, _i32, _vp, _u32]
+        L.gl_oracle_powers_by.restype = None
+        L.gl_oracle_omega_shift.argtypes = [_vp, _u32, _u32, _i32, _u32, _vp, _u32]
+        L.gl_oracle_omega_shift.restype = None
         _lib = L
     return _lib
 
@@ -103,6 +113,41 @@ def bitrev_permute(a: np.ndarray, log_n: int) -> np.ndarray:
     return a[..., rev.astype(np.int64)]
 
 
+def bit_reverse(src: np.ndarray, log_rows: int, cols: int, src_stride: int | None = None) -> np.ndarray:
+    """dst[brev(i)] = src[i] per column (src/ops_complex.rs:306-318); dense output (stride 2^log_rows)."""
+    rows = 1 << log_rows
+    src = np.ascontiguousarray(src, dtype=np.uint64)
+    dst = np.zeros(cols * rows, dtype=np.uint64)
+    lib().gl_oracle_bit_reverse(_p(src), src_stride if src_stride is not None else rows, _p(dst), rows, log_rows,
+                                cols)
+    return dst
+
+
+def powers_of(log_degree: int, offset: int, inverse: bool, bit_reverse: bool, of_g: bool, count: int) -> np.ndarray:
+    """get_powers_of_w / get_powers_of_g (native/ops_complex.cu:9-33), canonical."""
+    out = np.zeros(max(count, 1), dtype=np.uint64)
+    lib().gl_oracle_powers_of(log_degree, offset, int(inverse), int(bit_reverse), int(of_g), _p(out), count)
+    return out[:count]
+
+
+def powers_by(base, offset: int, bit_reverse: bool, count: int) -> np.ndarray:
+    """get_powers_by_val/ref (native/ops_complex.cu:35-74); base = int (base field) or (c0, c1) (extension,
+    result laid out as all c0 then all c1)."""
+    ext = isinstance(base, (tuple, list))
+    c0, c1 = (base[0], base[1]) if ext else (base, 0)
+    out = np.zeros(max((2 if ext else 1) * count, 1), dtype=np.uint64)
+    lib().gl_oracle_powers_by(c0, c1, int(ext), offset, int(bit_reverse), _p(out), count)
+    return out[:(2 if ext else 1) * count]
+
+
+def omega_shift(src: np.ndarray, log_degree: int, offset: int, inverse: bool, shift: int) -> np.ndarray:
+    """omega_shift (native/ops_complex.cu:76-87), canonical."""
+    src = np.ascontiguousarray(src, dtype=np.uint64)
+    out = np.zeros(max(len(src), 1), dtype=np.uint64)
+    lib().gl_oracle_omega_shift(_p(src), log_degree, offset, int(inverse), shift, _p(out), len(src))
+    return out[:len(src)]
+
+
 class RefKernels:
     """The reference's own CUDA NTT kernels (needs a GPU and oracle/_ref/libref_ntt.so)."""
 
@@ -117,6 +162,14 @@ class RefKernels:
         L.ref_batch_ntt.argtypes = [_vp, _vp, _u32, _u32, _u32, _u32, ctypes.c_bool, ctypes.c_bool, _u32, _u32,
                                     _vp]
         L.ref_batch_ntt.restype = _i32
+        L.ref_bit_reverse.argtypes = [_vp, _u64, _vp, _u64, _u32, _u32, _vp]
+        L.ref_bit_reverse.restype = _i32
+        L.ref_get_powers_of.argtypes = [_u32, _u32, ctypes.c_bool, ctypes.c_bool, ctypes.c_bool, _vp, _u32, _vp]
+        L.ref_get_powers_of.restype = _i32
+        L.ref_get_powers_by_val.argtypes = [_u64, _u64, ctypes.c_bool, _u32, ctypes.c_bool, _vp, _u32, _vp]
+        L.ref_get_powers_by_val.restype = _i32
+        L.ref_omega_shift.argtypes = [_vp, _u32, _u32, ctypes.c_bool, _u32, _vp, _u32, _vp]
+        L.ref_omega_shift.restype = _i32
         self.L = L
         rc = L.ref_context_create(12, 12)
         if rc != 0:
@@ -128,6 +181,31 @@ class RefKernels:
                                   log_ext, coset_idx, stream)
         if rc != 0:
             raise RuntimeError(f"ref_batch_ntt failed: {rc}")
+
+    def _ok(self, rc, what):
+        if rc != 0:
+            raise RuntimeError(f"{what} failed: {rc}")
+
+    def bit_reverse(self, src_ptr: int, src_stride: int, dst_ptr: int, dst_stride: int, log_rows: int, cols: int,
+                    stream: int):
+        self._ok(self.L.ref_bit_reverse(src_ptr, src_stride, dst_ptr, dst_stride, log_rows, cols, stream),
+                 "ref_bit_reverse")
+
+    def get_powers_of(self, log_degree: int, offset: int, inverse: bool, bit_reverse: bool, of_g: bool,
+                      result_ptr: int, count: int, stream: int):
+        self._ok(self.L.ref_get_powers_of(log_degree, offset, inverse, bit_reverse, of_g, result_ptr, count, stream),
+                 "ref_get_powers_of")
+
+    def get_powers_by_val(self, base, offset: int, bit_reverse: bool, result_ptr: int, count: int, stream: int):
+        ext = isinstance(base, (tuple, list))
+        c0, c1 = (base[0], base[1]) if ext else (base, 0)
+        self._ok(self.L.ref_get_powers_by_val(c0, c1, ext, offset, bit_reverse, result_ptr, count, stream),
+                 "ref_get_powers_by_val")
+
+    def omega_shift(self, src_ptr: int, log_degree: int, offset: int, inverse: bool, shift: int, dst_ptr: int,
+                    count: int, stream: int):
+        self._ok(self.L.ref_omega_shift(src_ptr, log_degree, offset, inverse, shift, dst_ptr, count, stream),
+                 "ref_omega_shift")
 
     def close(self):
         self.L.ref_context_destroy()

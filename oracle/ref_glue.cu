@@ -1,10 +1,11 @@
-// ref_glue.cu -- host glue that runs the REFERENCE's own NTT kernels.
+// ref_glue.cu -- host glue that runs the REFERENCE's own NTT and ops kernels.
 //
 // TEST / BASELINE INFRASTRUCTURE ONLY (never linked into the product).
 // oracle/Makefile (target `ref`) compiles this file together with the
-// reference's native/ntt.cu and native/context.cu, as separate translation
-// units read from where they lie in the reference checkout (nothing is
-// copied), with relocatable device code, into oracle/_ref/libref_ntt.so.
+// reference's native/ntt.cu, native/context.cu and native/ops_complex.cu, as
+// separate translation units read from where they lie in the reference
+// checkout (nothing is copied), with relocatable device code, into
+// oracle/_ref/libref_ntt.so.
 //
 // The reference's host side is Rust (src/context.rs, src/ntt.rs), which cannot
 // be built in this image (no Rust toolchain, boojum 0.2.2 not vendored), so
@@ -15,6 +16,8 @@
 //                             (PLANS table           src/ntt.rs:74-169,
 //                              launch geometry       src/ntt.rs:257-270,
 //                              per-stage path        src/ntt.rs:203-241)
+//   * ref_bit_reverse, ref_get_powers_of, ref_get_powers_by_val,
+//     ref_omega_shift      <- the wrappers of        src/ops_complex.rs:25-304
 // Roots of unity: boojum's domain_generator_for_size is replaced by the
 // generator-7 roots w_{2^k} = (7^((p-1)/2^32))^(2^(32-k)), the same choice the
 // C oracle (gl_oracle.c) and the product library make.
@@ -39,6 +42,34 @@ REF_NTT_KERNEL(b2n_initial_8_stages_warp)
 REF_NTT_KERNEL(b2n_initial_9_to_12_stages_block)
 REF_NTT_KERNEL(b2n_noninitial_7_or_8_stages_block)
 #undef REF_NTT_KERNEL
+
+// The reference's ops kernels (native/ops_complex.cu), declared with plain
+// structs of the same layout as its by-value parameters: matrix_getter /
+// matrix_setter = {T *ptr; size_t stride;} and vector_setter = {T *ptr;}
+// (native/memory.cuh:321-422), extension_field = 16-byte aligned pair
+// (native/goldilocks_extension.cuh:8-9).
+struct RefMat {
+  const void *ptr;
+  size_t stride;
+};
+struct RefVec {
+  void *ptr;
+};
+struct __align__(16) RefExt {
+  uint64_t c0, c1;
+};
+extern "C" __global__ void bit_reverse_naive_kernel(RefMat, RefMat, const unsigned);
+extern "C" __global__ void bit_reverse_kernel(RefMat, RefMat, const unsigned);
+extern "C" __global__ void get_powers_of_w_kernel(const unsigned, const unsigned, const bool, const bool, RefVec,
+                                                  const unsigned);
+extern "C" __global__ void get_powers_of_g_kernel(const unsigned, const unsigned, const bool, const bool, RefVec,
+                                                  const unsigned);
+extern "C" __global__ void get_powers_by_val_bf_kernel(const uint64_t, const unsigned, const bool, uint64_t *,
+                                                       const unsigned);
+extern "C" __global__ void get_powers_by_val_ef_kernel(const RefExt, const unsigned, const bool, RefExt *,
+                                                       const unsigned);
+extern "C" __global__ void omega_shift_kernel(const uint64_t *, const unsigned, const unsigned, const bool,
+                                              const unsigned, uint64_t *, const unsigned);
 
 #include <cstdint>
 #include <cstring>
@@ -257,4 +288,69 @@ extern "C" cudaError_t ref_batch_ntt(const uint64_t *inputs_ptr_in, uint64_t *ou
     if (e != cudaSuccess) return e;
   }
   return stage == log_n ? cudaSuccess : cudaErrorUnknown;
+}
+
+// ---------------------------------------------------------------- ops (src/ops_complex.rs)
+// Launch geometry of the reference's wrappers: get_launch_dims = 128-thread
+// blocks (src/ops_complex.rs:25-27, src/utils.rs:6-13).
+static dim3 ref_grid(unsigned count, unsigned &block) {
+  block = count < 128 ? (count ? count : 1) : 128;
+  return dim3((count + block - 1) / block);
+}
+
+// launch_bit_reverse (src/ops_complex.rs:271-304).
+extern "C" cudaError_t ref_bit_reverse(const uint64_t *src, uint64_t src_stride, uint64_t *dst, uint64_t dst_stride,
+                                       unsigned log_rows, unsigned cols, void *stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  const RefMat a{src, (size_t)src_stride}, b{dst, (size_t)dst_stride};
+  const unsigned half = log_rows >> 1;
+  if (half < 5) {
+    unsigned block;
+    dim3 grid = ref_grid(1u << log_rows, block);
+    grid.y = cols;
+    bit_reverse_naive_kernel<<<grid, block, 0, s>>>(a, b, log_rows);
+  } else {
+    const unsigned tiles = 1u << (half - 5);
+    const dim3 grid(tiles * (tiles + 1) / 2, log_rows - (half << 1) + 1, cols), block(32, 2, 2);
+    bit_reverse_kernel<<<grid, block, 0, s>>>(a, b, log_rows);
+  }
+  return cudaGetLastError();
+}
+
+// get_powers_of (src/ops_complex.rs:40-56); of_g selects get_powers_of_g.
+extern "C" cudaError_t ref_get_powers_of(unsigned log_degree, unsigned offset, bool inverse, bool bit_reverse,
+                                         bool of_g, uint64_t *result, unsigned count, void *stream) {
+  unsigned block;
+  const dim3 grid = ref_grid(count, block);
+  if (of_g)
+    get_powers_of_g_kernel<<<grid, block, 0, (cudaStream_t)stream>>>(log_degree, offset, inverse, bit_reverse,
+                                                                       RefVec{result}, count);
+  else
+    get_powers_of_w_kernel<<<grid, block, 0, (cudaStream_t)stream>>>(log_degree, offset, inverse, bit_reverse,
+                                                                       RefVec{result}, count);
+  return cudaGetLastError();
+}
+
+// get_powers_by_val (src/ops_complex.rs:117-131) for the base field (ext = false)
+// or the extension (result holds 2 * count words).
+extern "C" cudaError_t ref_get_powers_by_val(uint64_t base_c0, uint64_t base_c1, bool ext, unsigned offset,
+                                             bool bit_reverse, uint64_t *result, unsigned count, void *stream) {
+  unsigned block;
+  const dim3 grid = ref_grid(count, block);
+  if (ext)
+    get_powers_by_val_ef_kernel<<<grid, block, 0, (cudaStream_t)stream>>>(RefExt{base_c0, base_c1}, offset,
+                                                                            bit_reverse, (RefExt *)result, count);
+  else
+    get_powers_by_val_bf_kernel<<<grid, block, 0, (cudaStream_t)stream>>>(base_c0, offset, bit_reverse, result,
+                                                                            count);
+  return cudaGetLastError();
+}
+
+// omega_shift (src/ops_complex.rs:220-242).
+extern "C" cudaError_t ref_omega_shift(const uint64_t *src, unsigned log_degree, unsigned offset, bool inverse,
+                                       unsigned shift, uint64_t *dst, unsigned count, void *stream) {
+  unsigned block;
+  const dim3 grid = ref_grid(count, block);
+  omega_shift_kernel<<<grid, block, 0, (cudaStream_t)stream>>>(src, log_degree, offset, inverse, shift, dst, count);
+  return cudaGetLastError();
 }
