@@ -514,13 +514,15 @@ def run_large_section(reps: int = 5):
             "plain_hbm_frac": round(alg / (t_p / 1e3) / 1e9 / peak, 4), "bit_exact_fused_vs_plain": exact}
 
 
-def run_ops_section(ops, reps: int = 5):
+def run_ops_section(ops, reps: int = 5, note: str | None = None):
     """The ops beside the NTT (include/bc_ops.h; src/ops_complex.rs) on HBM-sized inputs.
 
-    `ops` maps an op name to a callable (src_ptr, dst_ptr, stream) -> None: this library's entry points in the
-    ours arm, the reference's own kernels in the reference arm, on the same workloads.  Every op is bound by
-    HBM traffic: 16 bytes per element for the bit reversal and the omega shift (read + write), 8 for the
-    powers (write only); achieved = those bytes / event-timed duration, frac of the measured copy peak.
+    `ops` maps an op name to a callable (src_ptr, dst_ptr, aux, stream) -> None: this library's entry points
+    in the ours arm, the reference's own kernels in the reference arm, on the same workloads (`aux`: pointers of
+    the smaller buffers).  Every op is bound by HBM traffic: 16 bytes per element for the bit reversal and the
+    omega shift (read + write), 8 for the powers (write only), 16 per extension coefficient written by the
+    barycentric precompute, 8 per value read by the barycentric evaluation (64 polynomials x 2^22 rows);
+    achieved = those bytes / event-timed duration, frac of the measured copy peak.
     """
     import torch
 
@@ -530,6 +532,13 @@ def run_ops_section(ops, reps: int = 5):
     a = torch.randint(-(2**63), 2**63 - 1, (n_vec,), device="cuda", dtype=torch.int64,
                       generator=torch.Generator(device="cuda").manual_seed(5))
     b = torch.empty_like(a)
+    small = {"x": torch.tensor([12345678901, 98765432109], dtype=torch.int64, device="cuda"),
+             "cf": torch.zeros(2, dtype=torch.int64, device="cuda"),
+             "coef": torch.zeros(2 << 24, dtype=torch.int64, device="cuda"),
+             "partial": torch.zeros(100 << 20, dtype=torch.int64, device="cuda"),
+             "evals": torch.zeros(128, dtype=torch.int64, device="cuda")}
+    aux = {k: v.data_ptr() for k, v in small.items()}
+    aux["partial_words"] = small["partial"].numel()
     stream = torch.cuda.current_stream()
     work = {  # name -> (elements, bytes per element, workload)
         "bit_reverse": (cols << log_rows, 16, f"{cols} cols x 2^{log_rows}, out of place"),
@@ -538,26 +547,31 @@ def run_ops_section(ops, reps: int = 5):
         "get_powers_of_w": (n_vec, 8, "2^28 elements, log_degree 24"),
         "get_powers_of_g": (n_vec, 8, "2^28 elements, log_degree 24"),
         "get_powers_by_val_bf": (n_vec, 8, "2^28 elements, base 42"),
+        "barycentric_precompute_at_ext": (1 << 24, 16, "2^24 coefficients at an extension point, bit-reversed"),
+        "batch_eval_base_at_base": (n_vec, 8, "64 polynomials x 2^22 rows at a base point"),
+        "batch_eval_base_at_ext": (n_vec, 8, "64 polynomials x 2^22 rows at an extension point"),
     }
     res = {}
     for name, fn in ops.items():
         elems, bpe, workload = work[name]
-        fn(a.data_ptr(), b.data_ptr(), stream.cuda_stream)
+        fn(a.data_ptr(), b.data_ptr(), aux, stream.cuda_stream)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(reps):
-            fn(a.data_ptr(), b.data_ptr(), stream.cuda_stream)
+            fn(a.data_ptr(), b.data_ptr(), aux, stream.cuda_stream)
         e1.record(stream)
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / reps
         gbs = elems * bpe / (ms / 1e3) / 1e9
         res[name] = {"workload": workload, "ms": round(ms, 4), "gelem_per_s": round(elems / (ms / 1e3) / 1e9, 2),
                      "achieved_gbs": round(gbs, 1), "hbm_frac": round(gbs / peak, 4)}
-    del a, b
+    del a, b, small
     torch.cuda.empty_cache()
     res["peak_gbs"] = peak
     res["peak_kind"] = peak_kind
+    if note:
+        res["note"] = note
     return res
 
 
@@ -572,25 +586,38 @@ def ops_ours():
         assert rc == 0, rc
 
     return {
-        "bit_reverse": lambda a, b, s: ck(L.bc_bit_reverse(a, rows, b, rows, 22, cols, s)),
-        "bit_reverse_in_place": lambda a, b, s: ck(L.bc_bit_reverse_in_place(a, rows, 22, cols, s)),
-        "omega_shift": lambda a, b, s: ck(L.bc_omega_shift(a, 24, 0, False, 3, b, n, s)),
-        "get_powers_of_w": lambda a, b, s: ck(L.bc_get_powers_of_w(24, 0, False, False, b, n, s)),
-        "get_powers_of_g": lambda a, b, s: ck(L.bc_get_powers_of_g(24, 0, False, False, b, n, s)),
-        "get_powers_by_val_bf": lambda a, b, s: ck(L.bc_get_powers_by_val_bf(42, 0, False, b, n, s)),
+        "bit_reverse": lambda a, b, x, s: ck(L.bc_bit_reverse(a, rows, b, rows, 22, cols, s)),
+        "bit_reverse_in_place": lambda a, b, x, s: ck(L.bc_bit_reverse_in_place(a, rows, 22, cols, s)),
+        "omega_shift": lambda a, b, x, s: ck(L.bc_omega_shift(a, 24, 0, False, 3, b, n, s)),
+        "get_powers_of_w": lambda a, b, x, s: ck(L.bc_get_powers_of_w(24, 0, False, False, b, n, s)),
+        "get_powers_of_g": lambda a, b, x, s: ck(L.bc_get_powers_of_g(24, 0, False, False, b, n, s)),
+        "get_powers_by_val_bf": lambda a, b, x, s: ck(L.bc_get_powers_by_val_bf(42, 0, False, b, n, s)),
+        "barycentric_precompute_at_ext": lambda a, b, x, s: ck(L.bc_precompute_lagrange_coeffs_at_ext(
+            x["x"], x["cf"], 7, x["coef"], 1 << 24, True, s)),
+        "batch_eval_base_at_base": lambda a, b, x, s: ck(L.bc_batch_eval(
+            0, a, rows, cols, x["coef"], x["partial"], x["partial_words"], None, 0, x["evals"], s)),
+        "batch_eval_base_at_ext": lambda a, b, x, s: ck(L.bc_batch_eval(
+            1, a, rows, cols, x["coef"], x["partial"], x["partial_words"], None, 0, x["evals"], s)),
     }
 
 
 def ops_reference(ref):
-    """The reference's own ops kernels (oracle.RefKernels), as run_ops_section callables."""
+    """The reference's own ops kernels (oracle.RefKernels), as run_ops_section callables.  Its batch_eval
+    is timed by its partial-reduce kernel alone: the column sums that follow are a CUB call on its Rust side."""
     rows, cols, n = 1 << 22, 64, 1 << 28
     return {
-        "bit_reverse": lambda a, b, s: ref.bit_reverse(a, rows, b, rows, 22, cols, s),
-        "bit_reverse_in_place": lambda a, b, s: ref.bit_reverse(a, rows, a, rows, 22, cols, s),
-        "omega_shift": lambda a, b, s: ref.omega_shift(a, 24, 0, False, 3, b, n, s),
-        "get_powers_of_w": lambda a, b, s: ref.get_powers_of(24, 0, False, False, False, b, n, s),
-        "get_powers_of_g": lambda a, b, s: ref.get_powers_of(24, 0, False, False, True, b, n, s),
-        "get_powers_by_val_bf": lambda a, b, s: ref.get_powers_by_val(42, 0, False, b, n, s),
+        "bit_reverse": lambda a, b, x, s: ref.bit_reverse(a, rows, b, rows, 22, cols, s),
+        "bit_reverse_in_place": lambda a, b, x, s: ref.bit_reverse(a, rows, a, rows, 22, cols, s),
+        "omega_shift": lambda a, b, x, s: ref.omega_shift(a, 24, 0, False, 3, b, n, s),
+        "get_powers_of_w": lambda a, b, x, s: ref.get_powers_of(24, 0, False, False, False, b, n, s),
+        "get_powers_of_g": lambda a, b, x, s: ref.get_powers_of(24, 0, False, False, True, b, n, s),
+        "get_powers_by_val_bf": lambda a, b, x, s: ref.get_powers_by_val(42, 0, False, b, n, s),
+        "barycentric_precompute_at_ext": lambda a, b, x, s: ref.barycentric_precompute(
+            True, x["x"], x["cf"], 7, x["coef"], 1 << 24, True, s),
+        "batch_eval_base_at_base": lambda a, b, x, s: ref.batch_eval_partial(0, a, rows, cols, x["coef"],
+                                                                          x["partial"], s),
+        "batch_eval_base_at_ext": lambda a, b, x, s: ref.batch_eval_partial(1, a, rows, cols, x["coef"],
+                                                                         x["partial"], s),
     }
 
 
@@ -711,7 +738,9 @@ def run_reference(args, rank, world):
     e2e_ms, _ = time_steps(e2e_step, e2e_steps, 1, world, stream)
     del dx, hx, hout, x, out, coef
     torch.cuda.empty_cache()
-    ops = run_ops_section(ops_reference(ref)) if world == 1 and not args.no_ops else None
+    ops = run_ops_section(ops_reference(ref), note="batch_eval_*: the reference's partial-reduce kernel only; "
+                          "the CUB column sums that its Rust side runs after it are not timed") \
+        if world == 1 and not args.no_ops else None
     line = {
         "metric": METRIC, "value": round(value, 1), "unit": "Melem/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,

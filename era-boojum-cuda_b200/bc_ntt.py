@@ -6,7 +6,8 @@ batch_ntt_out_of_place, batch_ntt_in_place}`` (src/ntt.rs:179-369) and
 This module exposes the same operations, with the same argument meaning, over
 the C ABI declared in include/bc_ntt.h, and the ops of src/ops_complex.rs
 (bit_reverse, get_powers_of_w/g, get_powers_by_val/ref, omega_shift) over
-include/bc_ops.h.  Device buffers are torch CUDA tensors
+include/bc_ops.h, and barycentric evaluation (src/barycentric.rs) over
+include/bc_barycentric.h.  Device buffers are torch CUDA tensors
 of dtype int64 or uint64 (the words are reinterpreted, never converted);
 streams default to torch's current stream.
 
@@ -82,6 +83,10 @@ SIGNATURES = {
     "bc_get_powers_by_ref_ef": [_vp, _u32, _b, _vp, _u32, _vp],
     "bc_omega_shift": [_vp, _u32, _u32, _b, _u32, _vp, _u32, _vp],
     "bc_omega_shift_in_place": [_vp, _u32, _u32, _b, _u32, _u32, _vp],
+    "bc_precompute_lagrange_coeffs_at_base": [_vp, _vp, _u64, _vp, _u32, _b, _vp],
+    "bc_precompute_lagrange_coeffs_at_ext": [_vp, _vp, _u64, _vp, _u32, _b, _vp],
+    "bc_get_batch_eval_temp_storage_sizes": [ctypes.c_int, _u32, _u32, _vp, _vp],
+    "bc_batch_eval": [ctypes.c_int, _vp, _u32, _u32, _vp, _vp, _sz, _vp, _sz, _vp, _vp],
 }
 
 CUDA_ERROR_NOT_READY = 600
@@ -443,3 +448,43 @@ def omega_shift_in_place(values, log_degree: int, offset: int, inverse: bool, sh
     n = _u32_count(_len(values), "omega_shift_in_place")
     _check(lib().bc_omega_shift_in_place(_ptr(values), log_degree, offset, inverse, shift, n, _stream(stream)),
            "omega_shift_in_place")
+
+
+# ---------------------------------------------------------------- barycentric (src/barycentric.rs, include/bc_barycentric.h)
+EVAL_BASE_AT_BASE, EVAL_BASE_AT_EXT, EVAL_EXT_AT_EXT = 0, 1, 2
+
+
+def precompute_lagrange_coeffs(x, common_factor_storage, coset: int, lagrange_coeffs, bit_reverse: bool,
+                               ext: bool = False, stream=None):
+    """precompute_lagrange_coeffs (src/barycentric.rs:83-126): x and common_factor_storage are device tensors
+    of 1 word (base field) or 2 words (extension, ext=True); lagrange_coeffs holds count (2 * count) words."""
+    w = 2 if ext else 1
+    if _len(x) < w or _len(common_factor_storage) < w:
+        raise ValueError("precompute_lagrange_coeffs: x / storage too short")
+    count = _len(lagrange_coeffs) // w
+    fn = lib().bc_precompute_lagrange_coeffs_at_ext if ext else lib().bc_precompute_lagrange_coeffs_at_base
+    _check(fn(_ptr(x), _ptr(common_factor_storage), coset, _ptr(lagrange_coeffs), count, bit_reverse,
+              _stream(stream)), "precompute_lagrange_coeffs")
+
+
+def get_batch_eval_temp_storage_sizes(kind: int, count: int, num_polys: int):
+    """get_batch_eval_temp_storage_sizes (src/barycentric.rs:193-209): (u64 words, bytes) of scratch."""
+    words, nbytes = ctypes.c_size_t(0), ctypes.c_size_t(0)
+    _check(lib().bc_get_batch_eval_temp_storage_sizes(kind, count, num_polys, ctypes.byref(words),
+                                                      ctypes.byref(nbytes)), "get_batch_eval_temp_storage_sizes")
+    return words.value, nbytes.value
+
+
+def batch_eval(kind: int, batch_ys, count: int, num_polys: int, lagrange_coeffs, temp_partial_reduce,
+               temp_final_reduce, evals, stream=None):
+    """batch_eval (src/barycentric.rs:211-260): evals[j] = sum_i ys[i, j] L_i for num_polys columns of count
+    rows; extension kinds write (c0, c1) pairs.  temp_final_reduce may be None (0 bytes needed)."""
+    xw = 1 if kind == EVAL_BASE_AT_BASE else 2
+    yw = 2 if kind == EVAL_EXT_AT_EXT else 1
+    if _len(batch_ys) < yw * num_polys * count or _len(lagrange_coeffs) < xw * count or _len(evals) < xw * num_polys:
+        raise ValueError("batch_eval: buffers too short")
+    fin_ptr = _ptr(temp_final_reduce) if temp_final_reduce is not None else None
+    fin_len = temp_final_reduce.numel() * temp_final_reduce.element_size() if temp_final_reduce is not None else 0
+    _check(lib().bc_batch_eval(kind, _ptr(batch_ys), count, num_polys, _ptr(lagrange_coeffs),
+                               _ptr(temp_partial_reduce), _len(temp_partial_reduce), fin_ptr, fin_len, _ptr(evals),
+                               _stream(stream)), "batch_eval")

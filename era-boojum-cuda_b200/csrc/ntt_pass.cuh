@@ -114,6 +114,15 @@ __device__ __forceinline__ uint64_t coset_power(const DevTables &t, uint32_t inv
   return r;
 }
 
+// w_{2^24}^e (inv = 1: w^-e) for e < 2^24, the reference's omega and index
+// convention (native/context.cuh:9-48): w_{2^24} = w_{2^PW_LOG}^(2^(PW_LOG-24)).
+__device__ __forceinline__ uint64_t w24_power(const DevTables &t, uint32_t inv, uint32_t e) {
+  const uint32_t e30 = e << (PW_LOG - 24);
+  const uint64_t w = ld_tab(t.w_lo[inv] + (e30 & ((1u << PW_FINE) - 1)));
+  const uint32_t eh = e30 >> PW_FINE;
+  return eh ? gl::mul(w, ld_tab(t.w_hi[inv] + eh)) : w;
+}
+
 __device__ __forceinline__ uint32_t pad16(uint32_t x) { return x + (x >> 4); }
 
 __device__ __forceinline__ uint32_t brev_bits(uint32_t x, uint32_t bits) { return bits ? __brev(x) >> (32 - bits) : 0; }

@@ -30,6 +30,7 @@
 #include <cstdint>
 
 #include "../../include/bc_ops.h"
+#include "ext.cuh"
 #include "ntt_host.cuh"
 #include "ntt_pass.cuh"
 
@@ -133,14 +134,6 @@ cudaError_t bit_reverse(const uint64_t *src, uint64_t ss, uint64_t *dst, uint64_
 }
 
 // ---------------------------------------------------------------- powers from the tables
-// w_{2^24}^e (inv: w^-e) for e < 2^24.
-__device__ __forceinline__ uint64_t w24_power(const DevTables &t, uint32_t inv, uint32_t e) {
-  const uint32_t e30 = e << (PW_LOG - 24);
-  uint64_t w = ld_tab(t.w_lo[inv] + (e30 & ((1u << PW_FINE) - 1)));
-  const uint32_t eh = e30 >> PW_FINE;
-  return eh ? gl::mul(w, ld_tab(t.w_hi[inv] + eh)) : w;
-}
-
 __device__ __forceinline__ uint64_t domain_power(const DevTables &t, uint32_t of_g, uint32_t inv, uint32_t e) {
   return of_g ? g_power(t, inv, e) : w24_power(t, inv, e);
 }
@@ -193,19 +186,6 @@ cudaError_t powers_of(uint32_t log_degree, uint32_t offset, bool inverse, bool b
 }
 
 // ---------------------------------------------------------------- powers of a base
-// Quadratic extension F_p[x] / (x^2 - 7).
-struct Ext {
-  uint64_t c0, c1;
-};
-
-__device__ __forceinline__ uint64_t mul7(uint64_t x) { return gl::sub(gl::mul_pow2<3>(x), x); }
-
-__device__ __forceinline__ Ext ext_mul(const Ext &a, const Ext &b) {
-  const uint64_t a0b0 = gl::mul(a.c0, b.c0), a1b1 = gl::mul(a.c1, b.c1);
-  const uint64_t cross = gl::mul(gl::add(a.c0, a.c1), gl::add(b.c0, b.c1)); // (a0 + a1)(b0 + b1)
-  return {gl::add(a0b0, mul7(a1b1)), gl::sub(gl::sub(cross, a0b0), a1b1)};
-}
-
 template <typename F> struct Arith;
 template <> struct Arith<uint64_t> {
   static __device__ __forceinline__ uint64_t one() { return 1; }

@@ -346,3 +346,101 @@ void gl_oracle_omega_shift(const uint64_t *src, unsigned log_degree, uint32_t of
     dst[i] = gl_mul(gl_canon(src[i]), gl_oracle_pow(w, e));
   }
 }
+
+/* ------------------------------------------------------------------ barycentric evaluation
+ * src/barycentric.rs, native/barycentric.cu: L_i(x) = cf * w^i / (x - c w^i),
+ * cf = c (x^N - c^N) / (N c^N), w = w_N, N = 2^log_count; x in the base field
+ * (ext = 0) or in F_p[x]/(x^2 - 7).  Element by element with a full inversion
+ * each (the reference's zero convention: inv(0) = 0). */
+
+static void ext_inv(const uint64_t a[2], uint64_t r[2]) {
+  /* (a0 + a1 x)^-1 = (a0 - a1 x) / (a0^2 - 7 a1^2) */
+  const uint64_t a0 = gl_canon(a[0]), a1 = gl_canon(a[1]);
+  const uint64_t nrm = gl_sub(gl_mul(a0, a0), gl_mul(7, gl_mul(a1, a1)));
+  const uint64_t ni = gl_oracle_inv(nrm);
+  r[0] = gl_mul(a0, ni);
+  r[1] = gl_sub(0, gl_mul(a1, ni));
+}
+
+/* out: N values (base) or 2N words, all c0 then all c1 (extension); natural
+ * order, bit-reversed when bit_reverse. */
+void gl_oracle_lagrange_coeffs(uint64_t x0, uint64_t x1, int ext, uint64_t coset, unsigned log_count, int bit_reverse,
+                               uint64_t *out) {
+  const uint64_t n = 1ull << log_count;
+  const uint64_t c = gl_canon(coset);
+  const uint64_t x[2] = {gl_canon(x0), ext ? gl_canon(x1) : 0};
+  uint64_t xn[2];
+  ext_pow(x, (uint32_t)n, xn); /* x^N; N <= 2^31 */
+  const uint64_t cn = gl_oracle_pow(c, n);
+  const uint64_t den_inv = gl_oracle_inv(gl_mul(n % GL_P, cn));
+  const uint64_t cf[2] = {gl_mul(gl_mul(gl_sub(xn[0], cn), c), den_inv), gl_mul(gl_mul(xn[1], c), den_inv)};
+  const uint64_t w = gl_oracle_root_of_unity(log_count);
+  uint64_t wi = 1;
+  for (uint64_t i = 0; i < n; i++) {
+    const uint64_t cw = gl_mul(c, wi);
+    const uint64_t d[2] = {gl_sub(x[0], cw), x[1]};
+    uint64_t di[2], l[2];
+    ext_inv(d, di);
+    const uint64_t cfw[2] = {gl_mul(cf[0], wi), gl_mul(cf[1], wi)};
+    ext_mul(cfw, di, l);
+    const uint64_t pos = bit_reverse ? brev((uint32_t)i, log_count) : i;
+    out[pos] = l[0];
+    if (ext) out[n + pos] = l[1];
+    wi = gl_mul(wi, w);
+  }
+}
+
+/* eval_j = sum_i y_{i,j} L_i.  kind 0: base values, base coefficients; 1: base
+ * values, extension coefficients; 2: extension values (column j = base columns
+ * 2j, 2j + 1) and extension coefficients.  out: one word (kind 0) or a (c0, c1)
+ * pair per polynomial. */
+void gl_oracle_batch_eval(int kind, const uint64_t *ys, uint32_t count, uint32_t num_polys, const uint64_t *coeffs,
+                          uint64_t *out) {
+  for (uint32_t j = 0; j < num_polys; j++) {
+    uint64_t acc[2] = {0, 0};
+    for (uint32_t i = 0; i < count; i++) {
+      uint64_t y[2], l[2], pr[2];
+      if (kind == 2) {
+        y[0] = gl_canon(ys[(uint64_t)2 * j * count + i]);
+        y[1] = gl_canon(ys[(uint64_t)(2 * j + 1) * count + i]);
+      } else {
+        y[0] = gl_canon(ys[(uint64_t)j * count + i]);
+        y[1] = 0;
+      }
+      l[0] = gl_canon(coeffs[i]);
+      l[1] = kind == 0 ? 0 : gl_canon(coeffs[count + i]);
+      ext_mul(y, l, pr);
+      acc[0] = gl_add(acc[0], pr[0]);
+      acc[1] = gl_add(acc[1], pr[1]);
+    }
+    if (kind == 0) {
+      out[j] = acc[0];
+    } else {
+      out[2 * j] = acc[0];
+      out[2 * j + 1] = acc[1];
+    }
+  }
+}
+
+/* sum_i a_{i,j} x^i for num_polys coefficient columns of count rows (Horner);
+ * x and the coefficients in the base field or the extension as above. */
+void gl_oracle_poly_eval(int ext_coeffs, const uint64_t *coeffs, uint32_t count, uint32_t num_polys, uint64_t x0,
+                         uint64_t x1, uint64_t *out) {
+  const uint64_t x[2] = {gl_canon(x0), gl_canon(x1)};
+  for (uint32_t j = 0; j < num_polys; j++) {
+    uint64_t acc[2] = {0, 0};
+    for (int64_t i = (int64_t)count - 1; i >= 0; i--) {
+      uint64_t t[2];
+      ext_mul(acc, x, t);
+      if (ext_coeffs) {
+        acc[0] = gl_add(t[0], gl_canon(coeffs[(uint64_t)2 * j * count + i]));
+        acc[1] = gl_add(t[1], gl_canon(coeffs[(uint64_t)(2 * j + 1) * count + i]));
+      } else {
+        acc[0] = gl_add(t[0], gl_canon(coeffs[(uint64_t)j * count + i]));
+        acc[1] = t[1];
+      }
+    }
+    out[2 * j] = acc[0];
+    out[2 * j + 1] = acc[1];
+  }
+}

@@ -6,9 +6,12 @@ cpu_baseline / reference legs of bench.py -- never by the product library.
 * ``batch_ntt`` / ``lde``: CPU restatement (gl_oracle.c) of src/ntt.rs:179-369
   semantics, numpy uint64 arrays in and out.
 * ``bit_reverse`` / ``powers_of`` / ``powers_by`` / ``omega_shift``: CPU
-  restatements (gl_oracle.c) of the ops in src/ops_complex.rs.
+  restatements (gl_oracle.c) of the ops in src/ops_complex.rs;
+  ``lagrange_coeffs`` / ``batch_eval`` / ``poly_eval``: barycentric evaluation
+  (src/barycentric.rs) and direct polynomial evaluation.
 * ``RefKernels``: the reference's own CUDA kernels (native/ntt.cu,
-  native/context.cu, native/ops_complex.cu) built into oracle/_ref/libref_ntt.so by
+  native/context.cu, native/ops_complex.cu, native/barycentric.cu) built into
+  oracle/_ref/libref_ntt.so by
   ``make -C oracle ref``, driven by ref_glue.cu's restatement of
   Context::create and batch_ntt_internal.
 """
@@ -55,6 +58,12 @@ def lib():
         L.gl_oracle_powers_by.restype = None
         L.gl_oracle_omega_shift.argtypes = [_vp, _u32, _u32, _i32, _u32, _vp, _u32]
         L.gl_oracle_omega_shift.restype = None
+        L.gl_oracle_lagrange_coeffs.argtypes = [_u64, _u64, _i32, _u64, _u32, _i32, _vp]
+        L.gl_oracle_lagrange_coeffs.restype = None
+        L.gl_oracle_batch_eval.argtypes = [_i32, _vp, _u32, _u32, _vp, _vp]
+        L.gl_oracle_batch_eval.restype = None
+        L.gl_oracle_poly_eval.argtypes = [_i32, _vp, _u32, _u32, _u64, _u64, _vp]
+        L.gl_oracle_poly_eval.restype = None
         _lib = L
     return _lib
 
@@ -148,6 +157,38 @@ def omega_shift(src: np.ndarray, log_degree: int, offset: int, inverse: bool, sh
     return out[:len(src)]
 
 
+EVAL_BASE_AT_BASE, EVAL_BASE_AT_EXT, EVAL_EXT_AT_EXT = 0, 1, 2
+
+
+def lagrange_coeffs(x, coset: int, log_count: int, bit_reverse: bool) -> np.ndarray:
+    """Barycentric coefficients L_i(x) on coset * <w_{2^log_count}> (src/barycentric.rs:83-126); x = int or
+    (c0, c1); extension result = all c0 then all c1."""
+    ext = isinstance(x, (tuple, list))
+    x0, x1 = (x[0], x[1]) if ext else (x, 0)
+    n = 1 << log_count
+    out = np.zeros((2 if ext else 1) * n, dtype=np.uint64)
+    lib().gl_oracle_lagrange_coeffs(x0, x1, int(ext), coset, log_count, int(bit_reverse), _p(out))
+    return out
+
+
+def batch_eval(kind: int, ys: np.ndarray, count: int, num_polys: int, coeffs: np.ndarray) -> np.ndarray:
+    """sum_i y_{i,j} L_i per column (src/barycentric.rs:211-260); (c0, c1) pairs for the extension kinds."""
+    ys = np.ascontiguousarray(ys, dtype=np.uint64)
+    coeffs = np.ascontiguousarray(coeffs, dtype=np.uint64)
+    out = np.zeros((1 if kind == EVAL_BASE_AT_BASE else 2) * max(num_polys, 1), dtype=np.uint64)
+    lib().gl_oracle_batch_eval(kind, _p(ys), count, num_polys, _p(coeffs), _p(out))
+    return out[:(1 if kind == EVAL_BASE_AT_BASE else 2) * num_polys]
+
+
+def poly_eval(coeffs: np.ndarray, count: int, num_polys: int, x, ext_coeffs: bool = False) -> np.ndarray:
+    """sum_i a_{i,j} x^i per column (Horner); (c0, c1) pairs per polynomial."""
+    coeffs = np.ascontiguousarray(coeffs, dtype=np.uint64)
+    x0, x1 = (x[0], x[1]) if isinstance(x, (tuple, list)) else (x, 0)
+    out = np.zeros(2 * max(num_polys, 1), dtype=np.uint64)
+    lib().gl_oracle_poly_eval(int(ext_coeffs), _p(coeffs), count, num_polys, x0, x1, _p(out))
+    return out[:2 * num_polys]
+
+
 class RefKernels:
     """The reference's own CUDA NTT kernels (needs a GPU and oracle/_ref/libref_ntt.so)."""
 
@@ -170,6 +211,12 @@ class RefKernels:
         L.ref_get_powers_by_val.restype = _i32
         L.ref_omega_shift.argtypes = [_vp, _u32, _u32, ctypes.c_bool, _u32, _vp, _u32, _vp]
         L.ref_omega_shift.restype = _i32
+        L.ref_barycentric_precompute.argtypes = [ctypes.c_bool, _vp, _vp, _u64, _vp, _u32, ctypes.c_bool, _vp]
+        L.ref_barycentric_precompute.restype = _i32
+        L.ref_batch_eval.argtypes = [_i32, _vp, _u32, _u32, _vp, _vp, _vp]
+        L.ref_batch_eval.restype = _i32
+        L.ref_batch_eval_partial.argtypes = [_i32, _vp, _u32, _u32, _vp, _vp, _vp]
+        L.ref_batch_eval_partial.restype = _i32
         self.L = L
         rc = L.ref_context_create(12, 12)
         if rc != 0:
@@ -206,6 +253,21 @@ class RefKernels:
                     count: int, stream: int):
         self._ok(self.L.ref_omega_shift(src_ptr, log_degree, offset, inverse, shift, dst_ptr, count, stream),
                  "ref_omega_shift")
+
+    def barycentric_precompute(self, ext: bool, x_ptr: int, cf_ptr: int, coset: int, coeffs_ptr: int, count: int,
+                               bit_reverse: bool, stream: int):
+        self._ok(self.L.ref_barycentric_precompute(ext, x_ptr, cf_ptr, coset, coeffs_ptr, count, bit_reverse, stream),
+                 "ref_barycentric_precompute")
+
+    def batch_eval(self, kind: int, ys_ptr: int, count: int, num_polys: int, coeffs_ptr: int, stream: int) -> np.ndarray:
+        out = np.zeros((1 if kind == 0 else 2) * max(num_polys, 1), dtype=np.uint64)
+        self._ok(self.L.ref_batch_eval(kind, ys_ptr, count, num_polys, coeffs_ptr, _p(out), stream), "ref_batch_eval")
+        return out[:(1 if kind == 0 else 2) * num_polys]
+
+    def batch_eval_partial(self, kind: int, ys_ptr: int, count: int, num_polys: int, coeffs_ptr: int,
+                           partial_ptr: int, stream: int):
+        self._ok(self.L.ref_batch_eval_partial(kind, ys_ptr, count, num_polys, coeffs_ptr, partial_ptr, stream),
+                 "ref_batch_eval_partial")
 
     def close(self):
         self.L.ref_context_destroy()

@@ -18,6 +18,9 @@
 //                              per-stage path        src/ntt.rs:203-241)
 //   * ref_bit_reverse, ref_get_powers_of, ref_get_powers_by_val,
 //     ref_omega_shift      <- the wrappers of        src/ops_complex.rs:25-304
+//   * ref_barycentric_precompute, ref_batch_eval
+//                          <- precompute_lagrange_coeffs, batch_eval
+//                                                    src/barycentric.rs:83-260
 // Roots of unity: boojum's domain_generator_for_size is replaced by the
 // generator-7 roots w_{2^k} = (7^((p-1)/2^32))^(2^(32-k)), the same choice the
 // C oracle (gl_oracle.c) and the product library make.
@@ -70,6 +73,24 @@ extern "C" __global__ void get_powers_by_val_ef_kernel(const RefExt, const unsig
                                                        const unsigned);
 extern "C" __global__ void omega_shift_kernel(const uint64_t *, const unsigned, const unsigned, const bool,
                                               const unsigned, uint64_t *, const unsigned);
+// native/barycentric.cu; ef_double_vector/matrix accessors wrap one matrix
+// accessor {ptr, stride} (native/memory.cuh:436-590), i.e. RefMat.
+extern "C" __global__ void barycentric_precompute_common_factor_bf_kernel(const uint64_t *, uint64_t *, const uint64_t,
+                                                                          const unsigned);
+extern "C" __global__ void barycentric_precompute_common_factor_ef_kernel(const RefExt *, RefExt *, const uint64_t,
+                                                                          const unsigned);
+extern "C" __global__ void barycentric_precompute_lagrange_coeffs_bf_kernel(const uint64_t *, const uint64_t *,
+                                                                            const uint64_t, const uint64_t, RefVec,
+                                                                            const unsigned);
+extern "C" __global__ void barycentric_precompute_lagrange_coeffs_ef_kernel(const RefExt *, const RefExt *,
+                                                                            const uint64_t, const uint64_t, RefMat,
+                                                                            const unsigned);
+extern "C" __global__ void batch_barycentric_partial_reduce_bf_bf_kernel(RefMat, RefVec, RefMat, const unsigned,
+                                                                         const unsigned);
+extern "C" __global__ void batch_barycentric_partial_reduce_bf_ef_kernel(RefMat, RefMat, RefMat, const unsigned,
+                                                                         const unsigned);
+extern "C" __global__ void batch_barycentric_partial_reduce_ef_ef_kernel(RefMat, RefMat, RefMat, const unsigned,
+                                                                         const unsigned);
 
 #include <cstdint>
 #include <cstring>
@@ -352,5 +373,107 @@ extern "C" cudaError_t ref_omega_shift(const uint64_t *src, unsigned log_degree,
   unsigned block;
   const dim3 grid = ref_grid(count, block);
   omega_shift_kernel<<<grid, block, 0, (cudaStream_t)stream>>>(src, log_degree, offset, inverse, shift, dst, count);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- barycentric (src/barycentric.rs)
+static uint64_t addp(uint64_t a, uint64_t b) {
+  a %= P;
+  b %= P;
+  const uint64_t s = a + b;
+  return (s < a || s >= P) ? s - P : s;
+}
+
+// precompute_lagrange_coeffs (src/barycentric.rs:83-126): the common-factor kernel, the coefficient kernel with
+// 128-thread blocks and INV_BATCH_SIZE 10 (base) / 6 (extension) elements per thread, w_inv_step =
+// w_N^-(128 * grid), then the optional bit reversal of the coefficient vector as a matrix of 1 (2) columns.
+extern "C" cudaError_t ref_barycentric_precompute(bool ext, const uint64_t *x, uint64_t *cf, uint64_t coset,
+                                                  uint64_t *coeffs, unsigned count, bool bit_reverse, void *stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  if (ext)
+    barycentric_precompute_common_factor_ef_kernel<<<1, 1, 0, s>>>((const RefExt *)x, (RefExt *)cf, coset, count);
+  else
+    barycentric_precompute_common_factor_bf_kernel<<<1, 1, 0, s>>>(x, cf, coset, count);
+  unsigned log_count = 0;
+  while ((1u << log_count) < count) log_count++;
+  const unsigned inv_batch = ext ? 6 : 10, block = 128;
+  const unsigned grid = (count + inv_batch * block - 1) / (inv_batch * block);
+  const uint64_t w_inv = inv(domain_generator(count));
+  const uint64_t w_inv_step = pw(w_inv, (uint64_t)block * grid);
+  if (ext)
+    barycentric_precompute_lagrange_coeffs_ef_kernel<<<grid, block, 0, s>>>(
+        (const RefExt *)x, (const RefExt *)cf, w_inv_step, coset, RefMat{coeffs, (size_t)count}, log_count);
+  else
+    barycentric_precompute_lagrange_coeffs_bf_kernel<<<grid, block, 0, s>>>(x, cf, w_inv_step, coset,
+                                                                            RefVec{coeffs}, log_count);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || !bit_reverse) return e;
+  return ref_bit_reverse(coeffs, count, coeffs, count, log_count, ext ? 2 : 1, stream);
+}
+
+// batch_eval (src/barycentric.rs:183-260): the partial-reduce kernel with blocks of 32 x 32 threads and 12
+// (base at base) / 6 elements per thread, then the column sums that the Rust side hands to CUB, done here
+// on the host; evals_host gets one word per polynomial (kind 0) or (c0, c1) pairs.  Synchronous.
+extern "C" cudaError_t ref_batch_eval(int kind, const uint64_t *ys, unsigned count, unsigned num_polys,
+                                      const uint64_t *coeffs, uint64_t *evals_host, void *stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  const unsigned ept = kind == 0 ? 12 : 6, bx = 32;
+  const unsigned grid = (count + ept * bx - 1) / (ept * bx);
+  const unsigned grid_size_x = bx * grid;
+  const unsigned rows = count < grid_size_x ? count : grid_size_x;
+  const unsigned xw = kind == 0 ? 1 : 2;
+  uint64_t *partial = nullptr;
+  cudaError_t e = cudaMalloc(&partial, (size_t)rows * num_polys * xw * sizeof(uint64_t));
+  if (e != cudaSuccess) return e;
+  unsigned log_count = 0;
+  while ((1u << log_count) < count) log_count++;
+  const dim3 block(bx, 32);
+  const RefMat y{ys, (size_t)count}, part{partial, (size_t)rows};
+  if (kind == 0)
+    batch_barycentric_partial_reduce_bf_bf_kernel<<<grid, block, 0, s>>>(y, RefVec{(void *)coeffs}, part, log_count,
+                                                                         num_polys);
+  else if (kind == 1)
+    batch_barycentric_partial_reduce_bf_ef_kernel<<<grid, block, 0, s>>>(y, RefMat{coeffs, (size_t)count}, part,
+                                                                         log_count, num_polys);
+  else
+    batch_barycentric_partial_reduce_ef_ef_kernel<<<grid, block, 0, s>>>(y, RefMat{coeffs, (size_t)count}, part,
+                                                                         log_count, num_polys);
+  e = cudaGetLastError();
+  std::vector<uint64_t> h((size_t)rows * num_polys * xw);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) e = cudaMemcpy(h.data(), partial, h.size() * sizeof(uint64_t), cudaMemcpyDeviceToHost);
+  cudaFree(partial);
+  if (e != cudaSuccess) return e;
+  // base-field column k of the partial matrix (extension: column j = base columns 2j, 2j + 1) -> evals[k]
+  for (size_t k = 0; k < (size_t)num_polys * xw; k++) {
+    uint64_t acc = 0;
+    for (unsigned r = 0; r < rows; r++) acc = addp(acc, h[k * rows + r]);
+    evals_host[k] = acc;
+  }
+  return cudaSuccess;
+}
+
+// The partial-reduce kernel of batch_eval alone (asynchronous), into `partial` of at least
+// min(count, 32 * grid) * num_polys * (1 or 2) words: what the reference runs on the GPU before the CUB
+// column sums (timing only).
+extern "C" cudaError_t ref_batch_eval_partial(int kind, const uint64_t *ys, unsigned count, unsigned num_polys,
+                                              const uint64_t *coeffs, uint64_t *partial, void *stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  const unsigned ept = kind == 0 ? 12 : 6, bx = 32;
+  const unsigned grid = (count + ept * bx - 1) / (ept * bx);
+  const unsigned rows = count < bx * grid ? count : bx * grid;
+  unsigned log_count = 0;
+  while ((1u << log_count) < count) log_count++;
+  const dim3 block(bx, 32);
+  const RefMat y{ys, (size_t)count}, part{partial, (size_t)rows};
+  if (kind == 0)
+    batch_barycentric_partial_reduce_bf_bf_kernel<<<grid, block, 0, s>>>(y, RefVec{(void *)coeffs}, part, log_count,
+                                                                         num_polys);
+  else if (kind == 1)
+    batch_barycentric_partial_reduce_bf_ef_kernel<<<grid, block, 0, s>>>(y, RefMat{coeffs, (size_t)count}, part,
+                                                                         log_count, num_polys);
+  else
+    batch_barycentric_partial_reduce_ef_ef_kernel<<<grid, block, 0, s>>>(y, RefMat{coeffs, (size_t)count}, part,
+                                                                         log_count, num_polys);
   return cudaGetLastError();
 }
