@@ -362,7 +362,7 @@ def run_ours(args, rank, world):
     if world == 1 and not args.no_serve:
         line["serve"] = run_serve_section()
     if world == 1 and not args.no_ops:
-        line["ops"] = run_ops_section(ops_ours())
+        line["ops"] = run_ops_section(ops_ours(), log_n=args.ops_log_n)
     return line
 
 
@@ -514,7 +514,7 @@ def run_large_section(reps: int = 5):
             "plain_hbm_frac": round(alg / (t_p / 1e3) / 1e9 / peak, 4), "bit_exact_fused_vs_plain": exact}
 
 
-def run_ops_section(ops, reps: int = 5, note: str | None = None):
+def run_ops_section(ops, reps: int = 5, note: str | None = None, log_n: int = 28):
     """The ops beside the NTT (include/bc_ops.h; src/ops_complex.rs) on HBM-sized inputs.
 
     `ops` maps an op name to a callable (src_ptr, dst_ptr, aux, stream) -> None: this library's entry points
@@ -527,29 +527,34 @@ def run_ops_section(ops, reps: int = 5, note: str | None = None):
     import torch
 
     peak, peak_kind = measured_peaks()
-    n_vec = 1 << 28                       # 2 GiB of u64, larger than L2
-    log_rows, cols = 22, 64               # bit reversal: 64 columns x 2^22 rows = 2 GiB
+    n_vec = 1 << log_n                    # 2 GiB of u64 at the default 2^28, larger than L2
+    log_rows, cols = 22, n_vec >> 22      # bit reversal / batch evaluation: cols x 2^22 rows
+    n_coef = 1 << min(24, log_n - 4)      # barycentric coefficients
     a = torch.randint(-(2**63), 2**63 - 1, (n_vec,), device="cuda", dtype=torch.int64,
                       generator=torch.Generator(device="cuda").manual_seed(5))
     b = torch.empty_like(a)
     small = {"x": torch.tensor([12345678901, 98765432109], dtype=torch.int64, device="cuda"),
              "cf": torch.zeros(2, dtype=torch.int64, device="cuda"),
-             "coef": torch.zeros(2 << 24, dtype=torch.int64, device="cuda"),
-             "partial": torch.zeros(100 << 20, dtype=torch.int64, device="cuda"),
+             "coef": torch.zeros(2 * max(n_coef, 1 << log_rows), dtype=torch.int64, device="cuda"),
+             # the reference's partial matrix: 32 * ceil(2^22 / 192) rows x cols x 2 words
+             "partial": torch.zeros(2 * cols * 32 * (((1 << log_rows) + 191) // 192), dtype=torch.int64,
+                                    device="cuda"),
              "evals": torch.zeros(128, dtype=torch.int64, device="cuda")}
     aux = {k: v.data_ptr() for k, v in small.items()}
     aux["partial_words"] = small["partial"].numel()
+    aux.update(n=n_vec, rows=1 << log_rows, log_rows=log_rows, cols=cols, n_coef=n_coef)
     stream = torch.cuda.current_stream()
     work = {  # name -> (elements, bytes per element, workload)
         "bit_reverse": (cols << log_rows, 16, f"{cols} cols x 2^{log_rows}, out of place"),
         "bit_reverse_in_place": (cols << log_rows, 16, f"{cols} cols x 2^{log_rows}, in place"),
-        "omega_shift": (n_vec, 16, "2^28 elements, log_degree 24, shift 3"),
-        "get_powers_of_w": (n_vec, 8, "2^28 elements, log_degree 24"),
-        "get_powers_of_g": (n_vec, 8, "2^28 elements, log_degree 24"),
-        "get_powers_by_val_bf": (n_vec, 8, "2^28 elements, base 42"),
-        "barycentric_precompute_at_ext": (1 << 24, 16, "2^24 coefficients at an extension point, bit-reversed"),
-        "batch_eval_base_at_base": (n_vec, 8, "64 polynomials x 2^22 rows at a base point"),
-        "batch_eval_base_at_ext": (n_vec, 8, "64 polynomials x 2^22 rows at an extension point"),
+        "omega_shift": (n_vec, 16, f"2^{log_n} elements, log_degree 24, shift 3"),
+        "get_powers_of_w": (n_vec, 8, f"2^{log_n} elements, log_degree 24"),
+        "get_powers_of_g": (n_vec, 8, f"2^{log_n} elements, log_degree 24"),
+        "get_powers_by_val_bf": (n_vec, 8, f"2^{log_n} elements, base 42"),
+        "barycentric_precompute_at_ext": (n_coef, 16, f"2^{min(24, log_n - 4)} coefficients at an extension point, "
+                                                       "bit-reversed"),
+        "batch_eval_base_at_base": (n_vec, 8, f"{cols} polynomials x 2^{log_rows} rows at a base point"),
+        "batch_eval_base_at_ext": (n_vec, 8, f"{cols} polynomials x 2^{log_rows} rows at an extension point"),
     }
     res = {}
     for name, fn in ops.items():
@@ -576,47 +581,47 @@ def run_ops_section(ops, reps: int = 5, note: str | None = None):
 
 
 def ops_ours():
-    """This library's ops, as run_ops_section callables."""
+    """This library's ops, as run_ops_section callables (sizes from aux)."""
     import bc_ntt
 
     L = bc_ntt.lib()
-    rows, cols, n = 1 << 22, 64, 1 << 28
 
     def ck(rc):
         assert rc == 0, rc
 
     return {
-        "bit_reverse": lambda a, b, x, s: ck(L.bc_bit_reverse(a, rows, b, rows, 22, cols, s)),
-        "bit_reverse_in_place": lambda a, b, x, s: ck(L.bc_bit_reverse_in_place(a, rows, 22, cols, s)),
-        "omega_shift": lambda a, b, x, s: ck(L.bc_omega_shift(a, 24, 0, False, 3, b, n, s)),
-        "get_powers_of_w": lambda a, b, x, s: ck(L.bc_get_powers_of_w(24, 0, False, False, b, n, s)),
-        "get_powers_of_g": lambda a, b, x, s: ck(L.bc_get_powers_of_g(24, 0, False, False, b, n, s)),
-        "get_powers_by_val_bf": lambda a, b, x, s: ck(L.bc_get_powers_by_val_bf(42, 0, False, b, n, s)),
+        "bit_reverse": lambda a, b, x, s: ck(L.bc_bit_reverse(a, x["rows"], b, x["rows"], x["log_rows"], x["cols"], s)),
+        "bit_reverse_in_place": lambda a, b, x, s: ck(L.bc_bit_reverse_in_place(a, x["rows"], x["log_rows"], x["cols"],
+                                                                                s)),
+        "omega_shift": lambda a, b, x, s: ck(L.bc_omega_shift(a, 24, 0, False, 3, b, x["n"], s)),
+        "get_powers_of_w": lambda a, b, x, s: ck(L.bc_get_powers_of_w(24, 0, False, False, b, x["n"], s)),
+        "get_powers_of_g": lambda a, b, x, s: ck(L.bc_get_powers_of_g(24, 0, False, False, b, x["n"], s)),
+        "get_powers_by_val_bf": lambda a, b, x, s: ck(L.bc_get_powers_by_val_bf(42, 0, False, b, x["n"], s)),
         "barycentric_precompute_at_ext": lambda a, b, x, s: ck(L.bc_precompute_lagrange_coeffs_at_ext(
-            x["x"], x["cf"], 7, x["coef"], 1 << 24, True, s)),
+            x["x"], x["cf"], 7, x["coef"], x["n_coef"], True, s)),
         "batch_eval_base_at_base": lambda a, b, x, s: ck(L.bc_batch_eval(
-            0, a, rows, cols, x["coef"], x["partial"], x["partial_words"], None, 0, x["evals"], s)),
+            0, a, x["rows"], x["cols"], x["coef"], x["partial"], x["partial_words"], None, 0, x["evals"], s)),
         "batch_eval_base_at_ext": lambda a, b, x, s: ck(L.bc_batch_eval(
-            1, a, rows, cols, x["coef"], x["partial"], x["partial_words"], None, 0, x["evals"], s)),
+            1, a, x["rows"], x["cols"], x["coef"], x["partial"], x["partial_words"], None, 0, x["evals"], s)),
     }
 
 
 def ops_reference(ref):
     """The reference's own ops kernels (oracle.RefKernels), as run_ops_section callables.  Its batch_eval
     is timed by its partial-reduce kernel alone: the column sums that follow are a CUB call on its Rust side."""
-    rows, cols, n = 1 << 22, 64, 1 << 28
     return {
-        "bit_reverse": lambda a, b, x, s: ref.bit_reverse(a, rows, b, rows, 22, cols, s),
-        "bit_reverse_in_place": lambda a, b, x, s: ref.bit_reverse(a, rows, a, rows, 22, cols, s),
-        "omega_shift": lambda a, b, x, s: ref.omega_shift(a, 24, 0, False, 3, b, n, s),
-        "get_powers_of_w": lambda a, b, x, s: ref.get_powers_of(24, 0, False, False, False, b, n, s),
-        "get_powers_of_g": lambda a, b, x, s: ref.get_powers_of(24, 0, False, False, True, b, n, s),
-        "get_powers_by_val_bf": lambda a, b, x, s: ref.get_powers_by_val(42, 0, False, b, n, s),
+        "bit_reverse": lambda a, b, x, s: ref.bit_reverse(a, x["rows"], b, x["rows"], x["log_rows"], x["cols"], s),
+        "bit_reverse_in_place": lambda a, b, x, s: ref.bit_reverse(a, x["rows"], a, x["rows"], x["log_rows"],
+                                                                   x["cols"], s),
+        "omega_shift": lambda a, b, x, s: ref.omega_shift(a, 24, 0, False, 3, b, x["n"], s),
+        "get_powers_of_w": lambda a, b, x, s: ref.get_powers_of(24, 0, False, False, False, b, x["n"], s),
+        "get_powers_of_g": lambda a, b, x, s: ref.get_powers_of(24, 0, False, False, True, b, x["n"], s),
+        "get_powers_by_val_bf": lambda a, b, x, s: ref.get_powers_by_val(42, 0, False, b, x["n"], s),
         "barycentric_precompute_at_ext": lambda a, b, x, s: ref.barycentric_precompute(
-            True, x["x"], x["cf"], 7, x["coef"], 1 << 24, True, s),
-        "batch_eval_base_at_base": lambda a, b, x, s: ref.batch_eval_partial(0, a, rows, cols, x["coef"],
+            True, x["x"], x["cf"], 7, x["coef"], x["n_coef"], True, s),
+        "batch_eval_base_at_base": lambda a, b, x, s: ref.batch_eval_partial(0, a, x["rows"], x["cols"], x["coef"],
                                                                           x["partial"], s),
-        "batch_eval_base_at_ext": lambda a, b, x, s: ref.batch_eval_partial(1, a, rows, cols, x["coef"],
+        "batch_eval_base_at_ext": lambda a, b, x, s: ref.batch_eval_partial(1, a, x["rows"], x["cols"], x["coef"],
                                                                          x["partial"], s),
     }
 
@@ -738,7 +743,8 @@ def run_reference(args, rank, world):
     e2e_ms, _ = time_steps(e2e_step, e2e_steps, 1, world, stream)
     del dx, hx, hout, x, out, coef
     torch.cuda.empty_cache()
-    ops = run_ops_section(ops_reference(ref), note="batch_eval_*: the reference's partial-reduce kernel only; "
+    ops = run_ops_section(ops_reference(ref), log_n=args.ops_log_n,
+                          note="batch_eval_*: the reference's partial-reduce kernel only; "
                           "the CUB column sums that its Rust side runs after it are not timed") \
         if world == 1 and not args.no_ops else None
     line = {
@@ -772,6 +778,7 @@ def main():
     ap.add_argument("--no-serve", action="store_true", help="skip the serving section")
     ap.add_argument("--no-large", action="store_true", help="skip the 64 x 2^23 blowup-4 section")
     ap.add_argument("--no-ops", action="store_true", help="skip the bit-reversal / powers / omega-shift section")
+    ap.add_argument("--ops-log-n", type=int, default=28, help="elements of the ops section's buffers (log2, >= 23)")
     ap.add_argument("--no-tuned-plans", action="store_true", help="ignore the autotuned plan file")
     ap.add_argument("--log-n", type=int, default=22, help="column length 2^log_n (default 22)")
     ap.add_argument("--cols", type=int, default=128, help="columns (default 128)")

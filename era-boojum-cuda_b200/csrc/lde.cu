@@ -209,7 +209,7 @@ cudaError_t launch_lde_step(const LdeStep &st, cudaStream_t stream) {
     }
     kern<<<st.grid, st.threads, st.smem, stream>>>(st.topp);
   } else {
-    PassKernel kern = pick_pass_kernel(st.K, st.C, st.b2n);
+    PassKernel kern = pick_pass_kernel(st.K, st.C, st.b2n, st.pass.inverse != 0);
     if (!kern) return cudaErrorInvalidValue;
     if (st.smem > 48 * 1024) {
       cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)st.smem);

@@ -223,47 +223,52 @@ bool plan_valid(const Plan &pl, uint32_t log_n) {
 
 // ---------------------------------------------------------------- kernels
 
-template <int K, int C, bool B2N> static PassKernel kptr() { return ntt_pass_kernel<K, C, B2N>; }
+template <int K, int C, bool B2N, bool INV> static PassKernel kptr() { return ntt_pass_kernel<K, C, B2N, INV>; }
 
-template <bool B2N> static PassKernel pick_c1(int K) {
+template <bool B2N, bool INV> static PassKernel pick_c1(int K) {
   switch (K) {
-  case 1: return kptr<1, 1, B2N>();
-  case 2: return kptr<2, 1, B2N>();
-  case 3: return kptr<3, 1, B2N>();
-  case 4: return kptr<4, 1, B2N>();
-  case 5: return kptr<5, 1, B2N>();
-  case 6: return kptr<6, 1, B2N>();
-  case 7: return kptr<7, 1, B2N>();
-  case 8: return kptr<8, 1, B2N>();
-  case 9: return kptr<9, 1, B2N>();
-  case 10: return kptr<10, 1, B2N>();
-  case 11: return kptr<11, 1, B2N>();
-  case 12: return kptr<12, 1, B2N>();
+  case 1: return kptr<1, 1, B2N, INV>();
+  case 2: return kptr<2, 1, B2N, INV>();
+  case 3: return kptr<3, 1, B2N, INV>();
+  case 4: return kptr<4, 1, B2N, INV>();
+  case 5: return kptr<5, 1, B2N, INV>();
+  case 6: return kptr<6, 1, B2N, INV>();
+  case 7: return kptr<7, 1, B2N, INV>();
+  case 8: return kptr<8, 1, B2N, INV>();
+  case 9: return kptr<9, 1, B2N, INV>();
+  case 10: return kptr<10, 1, B2N, INV>();
+  case 11: return kptr<11, 1, B2N, INV>();
+  case 12: return kptr<12, 1, B2N, INV>();
   default: return nullptr;
   }
 }
 
-template <bool B2N> static PassKernel pick_c8(int K) {
+template <bool B2N, bool INV> static PassKernel pick_c8(int K) {
   switch (K) {
-  case 1: return kptr<1, 8, B2N>();
-  case 2: return kptr<2, 8, B2N>();
-  case 3: return kptr<3, 8, B2N>();
-  case 4: return kptr<4, 8, B2N>();
-  case 5: return kptr<5, 8, B2N>();
-  case 6: return kptr<6, 8, B2N>();
-  case 7: return kptr<7, 8, B2N>();
-  case 8: return kptr<8, 8, B2N>();
-  case 9: return kptr<9, 8, B2N>();
+  case 1: return kptr<1, 8, B2N, INV>();
+  case 2: return kptr<2, 8, B2N, INV>();
+  case 3: return kptr<3, 8, B2N, INV>();
+  case 4: return kptr<4, 8, B2N, INV>();
+  case 5: return kptr<5, 8, B2N, INV>();
+  case 6: return kptr<6, 8, B2N, INV>();
+  case 7: return kptr<7, 8, B2N, INV>();
+  case 8: return kptr<8, 8, B2N, INV>();
+  case 9: return kptr<9, 8, B2N, INV>();
   default: return nullptr;
   }
 }
 
-PassKernel pick_pass_kernel(int K, int C, bool b2n) {
-  if (C == 1) return b2n ? pick_c1<true>(K) : pick_c1<false>(K);
-  if (C == 8) return b2n ? pick_c8<true>(K) : pick_c8<false>(K);
-  if (C == 4 && K == 10) return b2n ? kptr<10, 4, true>() : kptr<10, 4, false>();
-  if (C == 2 && K == 11) return b2n ? kptr<11, 2, true>() : kptr<11, 2, false>();
+template <bool B2N, bool INV> static PassKernel pick(int K, int C) {
+  if (C == 1) return pick_c1<B2N, INV>(K);
+  if (C == 8) return pick_c8<B2N, INV>(K);
+  if (C == 4 && K == 10) return kptr<10, 4, B2N, INV>();
+  if (C == 2 && K == 11) return kptr<11, 2, B2N, INV>();
   return nullptr;
+}
+
+PassKernel pick_pass_kernel(int K, int C, bool b2n, bool inverse) {
+  if (b2n) return inverse ? pick<true, true>(K, C) : pick<true, false>(K, C);
+  return inverse ? pick<false, true>(K, C) : pick<false, false>(K, C);
 }
 
 static uint32_t log2_ceil(uint64_t x) {
@@ -349,7 +354,7 @@ cudaError_t launch_pass(const PassLaunch &pl, cudaStream_t stream) {
   uint32_t threads;
   size_t smem;
   if (!build_pass(pl, 8, p, grid, threads, smem)) return cudaErrorInvalidConfiguration;
-  PassKernel kern = pick_pass_kernel(pl.K, pl.C, pl.b2n);
+  PassKernel kern = pick_pass_kernel(pl.K, pl.C, pl.b2n, pl.inverse);
   if (!kern) return cudaErrorInvalidValue;
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

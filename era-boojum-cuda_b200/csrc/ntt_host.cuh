@@ -59,8 +59,9 @@ bool build_pass(const PassLaunch &pl, int cols_factor_max, PassParams &p, dim3 &
                 size_t &smem_bytes);
 
 typedef void (*PassKernel)(const PassParams);
-// The standalone pass kernel for a window shape (nullptr when not instantiated).
-PassKernel pick_pass_kernel(int K, int C, bool b2n);
+// The standalone pass kernel for a window shape and twiddle direction (nullptr
+// when not instantiated).
+PassKernel pick_pass_kernel(int K, int C, bool b2n, bool inverse);
 
 // Window start (lowest bit) of pass i of a plan, passes listed top-down.
 uint32_t plan_lb(const Plan &pl, uint32_t log_n, int i);

@@ -45,8 +45,8 @@
 // Resident CTAs per SM the pass kernels are compiled for (256 threads each):
 // natural->bit-reversed passes 2 (128 registers a thread), bit-reversed->natural
 // ones 3 (80 registers; measured ~9 % faster on B200, while the n2b ones gain
-// nothing from the third CTA) except the windows of fewer than 9 bits with
-// runs of 8, which spill at 80 registers.
+// nothing from the third CTA) for windows of 9 bits and more (smaller windows
+// spill at 80 registers).
 #ifndef BC_PASS_MIN_BLOCKS
 #define BC_PASS_MIN_BLOCKS 2
 #endif
@@ -648,14 +648,14 @@ __device__ __forceinline__ void pass_body(const PassParams &p, uint32_t bx, uint
 // Shared memory (u64 words) of pass_body for a tile of `tile` elements.
 __host__ __device__ constexpr uint32_t pass_smem_words(uint32_t tile, int K) { return tile + tile / 16 + (1u << K); }
 
-template <int K, int C, bool B2N>
-__global__ void __launch_bounds__(256, (B2N && (K >= 9 || C == 1)) ? BC_PASS_MIN_BLOCKS_B2N : BC_PASS_MIN_BLOCKS)
+// One kernel per twiddle direction (INV == p.inverse, chosen on the host): a
+// kernel carrying both bodies behind a branch on p.inverse measured 4-10 us
+// slower per small launch in its second body.
+template <int K, int C, bool B2N, bool INV>
+__global__ void __launch_bounds__(256, (B2N && K >= 9) ? BC_PASS_MIN_BLOCKS_B2N : BC_PASS_MIN_BLOCKS)
     ntt_pass_kernel(const PassParams p) {
   extern __shared__ uint64_t smem[];
-  if (p.inverse)
-    pass_body<K, C, B2N, true>(p, blockIdx.x, blockIdx.y, smem);
-  else
-    pass_body<K, C, B2N, false>(p, blockIdx.x, blockIdx.y, smem);
+  pass_body<K, C, B2N, INV>(p, blockIdx.x, blockIdx.y, smem);
 }
 
 } // namespace bc
