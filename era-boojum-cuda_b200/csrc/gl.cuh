@@ -107,6 +107,44 @@ __device__ __forceinline__ uint64_t canon(uint64_t x) { return x >= P ? x - P : 
 
 __device__ __forceinline__ uint64_t mul(uint64_t a, uint64_t b) { return reduce128(a * b, __umul64hi(a, b)); }
 
+// reduce128 with a canonical result: t0 = lo - hh is formed as there; for
+// s = t0 + hl * EPS, a carry out of 2^64 leaves s - 2^64 + EPS < p, and
+// without one s >= p exactly when s + EPS carries (then s + EPS - 2^64 = s - p).
+__device__ __forceinline__ uint64_t reduce128_canon(uint64_t lo, uint64_t hi) {
+  uint64_t r;
+  asm("{\n\t"
+      ".reg .u32 l0, l1, hl, hh, t0, t1, u0, u1, v0, v1, c;\n\t"
+      ".reg .pred q;\n\t"
+      "mov.b64 {l0, l1}, %1;\n\t"
+      "mov.b64 {hl, hh}, %2;\n\t"
+      "sub.cc.u32 t0, l0, hh;\n\t"
+      "subc.cc.u32 t1, l1, 0;\n\t"
+      "subc.u32 c, 0, 0;\n\t"
+      "sub.cc.u32 t0, t0, c;\n\t"
+      "subc.u32 t1, t1, 0;\n\t"
+      "sub.cc.u32 u0, 0, hl;\n\t"
+      "subc.u32 u1, hl, 0;\n\t"
+      "add.cc.u32 t0, t0, u0;\n\t"
+      "addc.cc.u32 t1, t1, u1;\n\t"
+      "addc.u32 c, 0, 0;\n\t"
+      "add.cc.u32 v0, t0, 0xffffffff;\n\t"
+      "addc.cc.u32 v1, t1, 0;\n\t"
+      "addc.u32 c, c, 0;\n\t"
+      "setp.ne.u32 q, c, 0;\n\t"
+      "selp.b32 t0, v0, t0, q;\n\t"
+      "selp.b32 t1, v1, t1, q;\n\t"
+      "mov.b64 %0, {t0, t1};\n\t"
+      "}"
+      : "=l"(r)
+      : "l"(lo), "l"(hi));
+  return r;
+}
+
+// a * b reduced to [0, p).
+__device__ __forceinline__ uint64_t mul_canon(uint64_t a, uint64_t b) {
+  return reduce128_canon(a * b, __umul64hi(a, b));
+}
+
 // a + b (mod p) for b < p: a + b < 2^64 + p, so one carry correction suffices.
 __device__ __forceinline__ uint64_t add_bc(uint64_t a, uint64_t b) {
   uint64_t r;

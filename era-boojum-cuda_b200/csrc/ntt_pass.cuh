@@ -257,10 +257,14 @@ __device__ __forceinline__ void fill_powers(uint64_t *pw, const DevTables &tabs,
 }
 
 // Butterflies by the constant twiddle 2^E (E < 192).  DIT: the product is
-// reduced to [0, p), so the sum and difference need one correction each.
-template <int E> __device__ __forceinline__ void cdit(uint64_t &a, uint64_t &b) {
+// reduced to [0, p), so the sum and difference need one correction each;
+// with E = 0 the same holds when b is known canonical (BCAN).
+template <int E, bool BCAN = false> __device__ __forceinline__ void cdit(uint64_t &a, uint64_t &b) {
   const uint64_t a0 = a;
-  if constexpr (E == 0) {
+  if constexpr (E == 0 && BCAN) {
+    a = gl::add_bc(a0, b);
+    b = gl::sub_bc(a0, b);
+  } else if constexpr (E == 0) {
     a = gl::add(a0, b);
     b = gl::sub(a0, b);
   } else if constexpr (E < 96) {
@@ -286,7 +290,8 @@ template <int E> __device__ __forceinline__ void cdif(uint64_t &a, uint64_t &b) 
 }
 
 // One stage (bit QQ of a V-bit round) of the R = 0 network on x[OFF .. OFF + 2^V).
-template <bool DIF, bool INV, int V, int OFF, int QQ, int J0 = 0>
+// BCAN: the stage's second operands are canonical.
+template <bool DIF, bool INV, int V, int OFF, int QQ, bool BCAN, int J0 = 0>
 __device__ __forceinline__ void cstage(uint64_t (&x)[16]) {
   if constexpr (J0 < (1 << V)) {
     if constexpr (!(J0 & (1 << QQ))) {
@@ -294,17 +299,19 @@ __device__ __forceinline__ void cstage(uint64_t (&x)[16]) {
       if constexpr (DIF)
         cdif<E>(x[OFF + J0], x[OFF + (J0 | (1 << QQ))]);
       else
-        cdit<E>(x[OFF + J0], x[OFF + (J0 | (1 << QQ))]);
+        cdit<E, BCAN>(x[OFF + J0], x[OFF + (J0 | (1 << QQ))]);
     }
-    cstage<DIF, INV, V, OFF, QQ, J0 + 1>(x);
+    cstage<DIF, INV, V, OFF, QQ, BCAN, J0 + 1>(x);
   }
 }
 
 // The R = 0 network of a V-bit round: DIT top bit first, DIF bottom bit first.
+// DIT rounds enter with their upper half canonical (dit_prepare), so the
+// first stage -- all twiddles 1 -- takes one carry correction per add/sub.
 template <bool DIF, bool INV, int V, int OFF, int S = 0>
 __device__ __forceinline__ void cnet(uint64_t (&x)[16]) {
   if constexpr (S < V) {
-    cstage<DIF, INV, V, OFF, DIF ? S : V - 1 - S>(x);
+    cstage<DIF, INV, V, OFF, DIF ? S : V - 1 - S, !DIF && S == 0>(x);
     cnet<DIF, INV, V, OFF, S + 1>(x);
   }
 }
@@ -316,6 +323,23 @@ __device__ __forceinline__ void mul_powers(uint64_t (&x)[16], const uint64_t *pp
   for (int j = 1; j < (1 << V); j++) x[OFF + j] = gl::mul(x[OFF + j], pp[j - 1]);
 }
 
+// Entry of a DIT round: with scale, x[OFF + j] *= pp[j - 1] (the upper half
+// reduced to [0, p)); without, the upper half is only reduced.  Either way the
+// first stage's second operands are canonical (see cnet).
+template <int V, int OFF>
+__device__ __forceinline__ void dit_prepare(uint64_t (&x)[16], const uint64_t *pp, bool scale) {
+  constexpr int H = 1 << (V - 1);
+  if (scale) {
+#pragma unroll
+    for (int j = 1; j < H; j++) x[OFF + j] = gl::mul(x[OFF + j], pp[j - 1]);
+#pragma unroll
+    for (int j = H; j < 2 * H; j++) x[OFF + j] = gl::mul_canon(x[OFF + j], pp[j - 1]);
+  } else {
+#pragma unroll
+    for (int j = H; j < 2 * H; j++) x[OFF + j] = gl::canon(x[OFF + j]);
+  }
+}
+
 // One round of V bits at a compile-time offset B on every group of the thread.
 template <int K, int C, bool DIF, bool INV, int B, int V, int Q = 0>
 __device__ __forceinline__ void compute_groups(uint64_t (&x)[16], const uint64_t *pw, uint32_t tid,
@@ -325,7 +349,7 @@ __device__ __forceinline__ void compute_groups(uint64_t (&x)[16], const uint64_t
     uint32_t w;
     group_base<K, C, B, V>(tid + nthreads * Q, w);
     const uint64_t *pp = pw + ((1u << (K - B - V)) - 1) + (NV - 1) * (w >> (B + V));
-    if constexpr (!DIF) mul_powers<V, Q * NV>(x, pp);
+    if constexpr (!DIF) dit_prepare<V, Q * NV>(x, pp, true);
     cnet<DIF, INV, V, Q * NV>(x);
     if constexpr (DIF) mul_powers<V, Q * NV>(x, pp);
     compute_groups<K, C, DIF, INV, B, V, Q + 1>(x, pw, tid, nthreads);
@@ -386,7 +410,7 @@ __device__ __forceinline__ void slots16(uint32_t eb, uint32_t S, uint32_t (&a)[1
 template <int K, bool DIF, bool INV>
 __device__ __forceinline__ void net16(uint64_t (&x)[16], const uint64_t *pw, uint32_t w, uint32_t B, bool scale) {
   const uint64_t *pp = pw + ((1u << (K - 4 - B)) - 1) + 15 * (w >> (B + 4));
-  if (!DIF && scale) mul_powers<4, 0>(x, pp);
+  if constexpr (!DIF) dit_prepare<4, 0>(x, pp, scale);
   cnet<DIF, INV, 4, 0>(x);
   if (DIF && scale) mul_powers<4, 0>(x, pp);
 }
