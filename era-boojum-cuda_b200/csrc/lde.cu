@@ -164,8 +164,24 @@ bool build_lde_steps(const Plan &pl, const uint64_t *in, uint64_t *out, uint32_t
     const uint32_t tile = G << wc_log;
     st.threads = tile / 16;
     const uint32_t nb = 1u << log_blowup;
-    p.fwd_resident = (size_t)top_smem_words(tile, K, nb) * sizeof(uint64_t) <= TOP_RESIDENT_SMEM_MAX ? 1 : 0;
-    st.smem = (size_t)top_smem_words(tile, K, p.fwd_resident ? nb : 1) * sizeof(uint64_t);
+    // forward power tables: all resident if they fit with two CTAs per SM, else
+    // two slots fed ahead by cp.async from the precomputed ones, else refilled
+    p.fwd_tables = top_power_tables((uint32_t)K, log_blowup, false);
+    p.inv_table = top_power_tables((uint32_t)K, log_blowup, true);
+    auto fits = [&](uint32_t tables) {
+      return (size_t)top_smem_words(tile, K, tables) * sizeof(uint64_t) <= TOP_RESIDENT_SMEM_MAX;
+    };
+    uint32_t slots = 1;
+    if (fits(nb)) {
+      p.fwd_mode = TOP_TABLES_RESIDENT;
+      slots = nb;
+    } else if (p.fwd_tables && K >= 4 && fits(2)) {
+      p.fwd_mode = TOP_TABLES_PREFETCH;
+      slots = 2;
+    } else {
+      p.fwd_mode = TOP_TABLES_REFILL;
+    }
+    st.smem = (size_t)top_smem_words(tile, K, slots) * sizeof(uint64_t);
     const uint64_t gy = (num_cols + p.cols_per_cta - 1) / p.cols_per_cta;
     if (gy > 65535 || tiles > 0x7fffffffull) return false;
     st.grid = dim3((uint32_t)tiles, (uint32_t)gy);

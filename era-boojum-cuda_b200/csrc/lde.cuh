@@ -13,6 +13,33 @@
 
 namespace bc {
 
+enum : uint32_t { TOP_TABLES_REFILL = 0, TOP_TABLES_RESIDENT = 1, TOP_TABLES_PREFETCH = 2 };
+
+// Word offset of the power tables after a padded tile, rounded up to an even
+// word so that 16-byte copies into them are aligned.
+__host__ __device__ constexpr uint32_t top_tables_offset(uint32_t tile) { return (tile + tile / 16 + 1) & ~1u; }
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Copies a 2^K-word power table (16-byte aligned both sides) into shared memory:
+// plain 16-byte loads, or cp.async (ASYNC: completion by cp_async_wait).
+template <int K, bool ASYNC>
+__device__ __forceinline__ void copy_table(uint64_t *dst, const uint64_t *src, uint32_t tid, uint32_t nthreads) {
+  for (uint32_t c = tid; c < (1u << (K - 1)); c += nthreads) {
+    if constexpr (ASYNC)
+      cp_async16(dst + 2 * c, src + 2 * c);
+    else
+      reinterpret_cast<ulonglong2 *>(dst)[c] = __ldg(reinterpret_cast<const ulonglong2 *>(src) + c);
+  }
+}
+
 struct LdeTopParams {
   const uint64_t *in; // T (or the evaluations when the plan has one pass)
   uint64_t *out;      // coset block 0
@@ -27,7 +54,13 @@ struct LdeTopParams {
   uint32_t cols_per_cta;
   uint32_t canon_out; // single-pass plan: this kernel writes final values
   uint32_t vec_in, vec_out;
-  uint32_t fwd_resident; // the forward power tables of all cosets stay in shared memory
+  // forward power tables in shared memory: TOP_TABLES_RESIDENT (all cosets',
+  // filled once per CTA), TOP_TABLES_PREFETCH (two slots, the next coset's
+  // table copied with cp.async from fwd_tables during this coset's rounds) or
+  // TOP_TABLES_REFILL (one slot, computed again for every coset)
+  uint32_t fwd_mode;
+  const uint64_t *fwd_tables; // precomputed forward tables of the cosets (or nullptr)
+  const uint64_t *inv_table;  // precomputed inverse table (or nullptr)
   DevTables tabs;
 };
 
@@ -70,22 +103,34 @@ __device__ __forceinline__ void top_body(const LdeTopParams &p, uint32_t bx, uin
   const uint32_t TILE = G * W * C;
   const uint32_t T = TILE / 16;
   uint64_t *tile = smem;
-  // power tables (ntt_pass.cuh): the inverse one, then one forward table per
-  // coset (fwd_resident, filled once per CTA) or one refilled for every coset
-  uint64_t *pw_inv = smem + TILE + TILE / 16;
+  // power tables (ntt_pass.cuh): the inverse one, then the forward ones of
+  // fwd_mode (see LdeTopParams)
+  uint64_t *pw_inv = smem + top_tables_offset(TILE); // 16-byte aligned: tables are copied 16 bytes at a time
   uint64_t *pw_fwd = pw_inv + PowWords<K>::words;
+  constexpr uint32_t PW = PowWords<K>::words;
   const uint32_t tid = threadIdx.x;
 
   // top window: H = 0, the tile position is the run of low positions
   const uint64_t base_off = (uint64_t)bx << LogC<C>::v;
   const uint32_t col_begin = by * p.cols_per_cta;
   const uint32_t col_end = min(p.num_cols, col_begin + p.cols_per_cta);
-  fill_powers<K>(pw_inv, p.tabs, 1, 0, tid, T);
   const uint32_t nb = 1u << p.log_blowup;
-  if (p.fwd_resident)
-    for (uint32_t k = 0; k < nb; k++)
-      fill_powers<K>(pw_fwd + k * PowWords<K>::words, p.tabs, 0, brev_bits(k, p.log_blowup), tid, T,
-                     (k + 1) * PowWords<K>::tasks);
+  if (p.inv_table)
+    copy_table<K, false>(pw_inv, p.inv_table, tid, T);
+  else
+    fill_powers<K>(pw_inv, p.tabs, 1, 0, tid, T);
+  if (p.fwd_mode == TOP_TABLES_RESIDENT) {
+    for (uint32_t k = 0; k < nb; k++) {
+      if (p.fwd_tables)
+        copy_table<K, false>(pw_fwd + k * PW, p.fwd_tables + k * PW, tid, T);
+      else
+        fill_powers<K>(pw_fwd + k * PW, p.tabs, 0, brev_bits(k, p.log_blowup), tid, T, (k + 1) * PowWords<K>::tasks);
+    }
+  } else if (p.fwd_mode == TOP_TABLES_PREFETCH) {
+    copy_table<K, true>(pw_fwd, p.fwd_tables, tid, T); // coset 0 of the first column
+    cp_async_commit();
+  }
+  uint32_t step = 0; // cosets done so far: PREFETCH keeps step's table in slot step & 1
   // the column loop's first barrier orders these fills before any use
 
   const uint64_t inv_n = p.tabs.inv_pow2[p.log_n];
@@ -138,8 +183,8 @@ __device__ __forceinline__ void top_body(const LdeTopParams &p, uint32_t bx, uin
       }
       for (uint32_t k = 0; k < nb; k++) {
         __syncthreads();
-        const uint64_t *pwk = pw_fwd + (p.fwd_resident ? k * PowWords<K>::words : 0);
-        if (!p.fwd_resident) {
+        const uint64_t *pwk = pw_fwd + (p.fwd_mode == TOP_TABLES_RESIDENT ? k * PW : 0);
+        if (p.fwd_mode != TOP_TABLES_RESIDENT) { // windows under 4 bits never prefetch
           fill_powers<K>(pw_fwd, p.tabs, 0, brev_bits(k, p.log_blowup), tid, T);
           __syncthreads();
         }
@@ -192,11 +237,23 @@ __device__ __forceinline__ void top_body(const LdeTopParams &p, uint32_t bx, uin
       }
       for (uint32_t k = 0; k < nb; k++) {
         __syncthreads(); // previous coset's stores have read the tile (and the powers)
-        const uint64_t *pwk = pw_fwd + (p.fwd_resident ? k * PowWords<K>::words : 0);
-        if (!p.fwd_resident) {
+        const uint64_t *pwk = pw_fwd;
+        if (p.fwd_mode == TOP_TABLES_RESIDENT) {
+          pwk = pw_fwd + k * PW;
+        } else if (p.fwd_mode == TOP_TABLES_PREFETCH) {
+          // the slot of the previous step is free: start the next step's copy,
+          // then wait for this step's (all but the newest group)
+          pwk = pw_fwd + (step & 1) * PW;
+          const bool more = k + 1 < nb || c0 + G < col_end;
+          if (more) copy_table<K, true>(pw_fwd + ((step + 1) & 1) * PW, p.fwd_tables + ((k + 1) % nb) * PW, tid, T);
+          cp_async_commit();
+          cp_async_wait<1>();
+          __syncthreads();
+        } else {
           fill_powers<K>(pw_fwd, p.tabs, 0, brev_bits(k, p.log_blowup), tid, T);
           __syncthreads();
         }
+        step++;
         // forward stages (top-down): the first full round starts from the registers
         // (its R is the coset prefix brev(k): s = 1 for k = 0)
 #pragma unroll 1
@@ -225,12 +282,13 @@ __device__ __forceinline__ void top_body(const LdeTopParams &p, uint32_t bx, uin
     }
     __syncthreads();
   }
+  if (p.fwd_mode == TOP_TABLES_PREFETCH) cp_async_wait<0>(); // nothing in flight past the body
 }
 
 // Shared memory (u64 words) of top_body: tile, padding, the inverse power
-// table and fwd_tables forward ones.
+// table and fwd_tables forward ones (or slots).
 __host__ __device__ constexpr uint32_t top_smem_words(uint32_t tile, int K, uint32_t fwd_tables) {
-  return tile + tile / 16 + (1 + fwd_tables) * (1u << K);
+  return top_tables_offset(tile) + (1 + fwd_tables) * (1u << K);
 }
 
 // Largest shared memory of a top-window kernel whose forward tables stay

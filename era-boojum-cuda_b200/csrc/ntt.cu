@@ -45,6 +45,7 @@ constexpr int MAX_DEVICES = 64;
 struct DeviceCtx {
   bool live = false;
   uint64_t *block = nullptr;
+  uint64_t *top_pw = nullptr; // precomputed top-window power tables
   DevTables tabs{};
   int sms = 0;
 };
@@ -55,6 +56,7 @@ constexpr size_t N_TW_LO = 1u << TW_FINE, N_TW_HI = 1u << (TW_LOG - 1 - TW_FINE)
 constexpr size_t N_G_LO = 1u << G_FINE, N_G_HI = 1u << (TW_LOG - G_FINE);
 constexpr size_t N_W_LO = 1u << PW_FINE, N_W_HI = 1u << (PW_LOG - PW_FINE);
 constexpr size_t TABLE_WORDS = 2 * (N_TW_LO + N_TW_HI + N_G_LO + N_G_HI + N_W_LO + N_W_HI);
+constexpr int MAX_TOP_K = 12; // largest window of a pass
 
 void build_host_tables(std::vector<uint64_t> &h, size_t off[12]) {
   using namespace hostf;
@@ -113,6 +115,32 @@ int sm_count() {
   return n;
 }
 
+// Layout of the top-window power tables: per K (1..12) the inverse table, then
+// for b = 1 .. TOP_PW_LOG - K the 2^b forward tables, 2^K words each, i.e.
+// 2^K (2^(TOP_PW_LOG + 1 - K) - 1) = 2^16 - 2^K words per K.  Table t of a K
+// (t = 0 the inverse one, t = 2^b - 1 + k the forward one of coset k of b).
+size_t top_pw_base(int K) { return (size_t)(K - 1) * (1u << (TOP_PW_LOG + 1)) - ((1u << K) - 2); }
+size_t top_pw_words() { return top_pw_base(MAX_TOP_K + 1); }
+
+// One block per table t of window size K.
+template <int K> __global__ void top_pw_fill_kernel(const DevTables tabs, uint64_t *base) {
+  const uint32_t t = blockIdx.x;
+  uint32_t inv = 1, H = 0;
+  if (t > 0) {
+    const uint32_t b = 31 - __clz(t + 1), k = t + 1 - (1u << b);
+    inv = 0;
+    H = brev_bits(k, b);
+  }
+  fill_powers<K>(base + (size_t)t * (1u << K), tabs, inv, H, threadIdx.x, blockDim.x);
+}
+
+template <int K> cudaError_t top_pw_fill(const DevTables &tabs, uint64_t *all) {
+  const uint32_t tables = (1u << (TOP_PW_LOG + 1 - K)) - 1;
+  top_pw_fill_kernel<K><<<tables, 256>>>(tabs, all + top_pw_base(K));
+  if constexpr (K < MAX_TOP_K) return top_pw_fill<K + 1>(tabs, all);
+  return cudaGetLastError();
+}
+
 cudaError_t context_create_current() {
   std::lock_guard<std::mutex> lock(g_ctx_mutex);
   const int d = current_device();
@@ -145,9 +173,27 @@ cudaError_t context_create_current() {
   const uint64_t two_inv = hostf::inv(2);
   uint64_t acc = 1;
   for (int k = 0; k <= TW_LOG; k++, acc = hostf::mul(acc, two_inv)) c.tabs.inv_pow2[k] = acc;
+  e = cudaMalloc(&c.top_pw, top_pw_words() * sizeof(uint64_t));
+  if (e == cudaSuccess) e = top_pw_fill<1>(c.tabs, c.top_pw);
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) {
+    cudaFree(c.block);
+    cudaFree(c.top_pw);
+    c.block = c.top_pw = nullptr;
+    return e;
+  }
   cudaDeviceGetAttribute(&c.sms, cudaDevAttrMultiProcessorCount, d);
   c.live = true;
   return cudaSuccess;
+}
+
+const uint64_t *top_power_tables(uint32_t K, uint32_t log_blowup, bool inverse) {
+  const int d = current_device();
+  if (d < 0 || d >= MAX_DEVICES || !g_ctx[d].live || K < 1 || K > (uint32_t)MAX_TOP_K) return nullptr;
+  const uint64_t *base = g_ctx[d].top_pw + top_pw_base((int)K);
+  if (inverse) return base;
+  if (log_blowup < 1 || K + log_blowup > (uint32_t)TOP_PW_LOG) return nullptr;
+  return base + ((size_t)(1u << log_blowup) - 1) * (1u << K);
 }
 
 cudaError_t context_destroy_current() {
@@ -158,7 +204,9 @@ cudaError_t context_destroy_current() {
   if (!c.live) return cudaSuccess;
   c.live = false;
   cudaError_t e = cudaFree(c.block);
-  c.block = nullptr;
+  const cudaError_t e2 = cudaFree(c.top_pw);
+  if (e == cudaSuccess) e = e2;
+  c.block = c.top_pw = nullptr;
   return e;
 }
 

@@ -51,7 +51,7 @@ def test_lde_small_sizes(gpu_ctx, fused, log_b):
         np.testing.assert_array_equal(got, exp, err_msg=f"log_n={log_n} B={1 << log_b} fused={fused}")
 
 
-@pytest.mark.parametrize("log_n,cols,log_b", [(17, 5, 1), (20, 3, 2), (22, 2, 1), (23, 1, 2), (21, 9, 3)])
+@pytest.mark.parametrize("log_n,cols,log_b", [(17, 5, 1), (20, 3, 2), (22, 2, 1), (23, 1, 2), (21, 9, 3), (22, 2, 3)])
 def test_lde_large_sizes(gpu_ctx, log_n, cols, log_b):
     rng = np.random.default_rng(log_n)
     n = 1 << log_n
