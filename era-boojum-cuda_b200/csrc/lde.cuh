@@ -19,15 +19,6 @@ enum : uint32_t { TOP_TABLES_REFILL = 0, TOP_TABLES_RESIDENT = 1, TOP_TABLES_PRE
 // word so that 16-byte copies into them are aligned.
 __host__ __device__ constexpr uint32_t top_tables_offset(uint32_t tile) { return (tile + tile / 16 + 1) & ~1u; }
 
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
-  const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N> __device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-
 // Copies a 2^K-word power table (16-byte aligned both sides) into shared memory:
 // plain 16-byte loads, or cp.async (ASYNC: completion by cp_async_wait).
 template <int K, bool ASYNC>

@@ -125,6 +125,21 @@ __device__ __forceinline__ uint64_t w24_power(const DevTables &t, uint32_t inv, 
 
 __device__ __forceinline__ uint32_t pad16(uint32_t x) { return x + (x >> 4); }
 
+// Asynchronous global -> shared copies (cp.async); completion by cp_async_wait
+// (then a barrier before other threads read the data).
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
+  const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 __device__ __forceinline__ uint32_t brev_bits(uint32_t x, uint32_t bits) { return bits ? __brev(x) >> (32 - bits) : 0; }
 
 // ---------------------------------------------------------------- factored rounds
@@ -504,7 +519,10 @@ __device__ __forceinline__ void pass_body(const PassParams &p, uint32_t bx, uint
   const uint32_t tid = threadIdx.x;
   const TileGeom tg = tile_geom<K, C>(p, bx, by);
   const uint32_t Hbig = tg.H + (brev_bits(tg.group, p.log_groups) << (p.log_n - p.lb - K));
-  fill_powers<K>(pw, p.tabs, INV, Hbig, tid, T);
+  // Bit-reversed -> natural passes fill the power table in their first column
+  // group while that group's tile copy is in flight (cp.async); the others
+  // fill it here.
+  if constexpr (!B2N && NF > 0) fill_powers<K>(pw, p.tabs, INV, Hbig, tid, T);
   const bool top_s = Hbig != 0; // the top round's s differs from 1
 
   const uint64_t *in = p.in + tg.group * p.group_stride_in;
@@ -557,6 +575,9 @@ __device__ __forceinline__ void pass_body(const PassParams &p, uint32_t bx, uint
       full_rounds<K, C, false, INV>(tile, pw, (int)B - 4, -4, NF - 1, tid);
       if constexpr (R > 0) rounds_from<K, C, false, INV, false, NF>(tile, pw, tid, T);
     } else {
+      // the tile: a plain copy goes by cp.async (8-byte: padded slots are only
+      // 8-byte aligned), completed after the first group's table fill
+      const bool async_copy = !p.load_scale;
 #pragma unroll
       for (int j = 0; j < 8; j++) {
         const uint32_t e = 2 * (tid + T * j);
@@ -564,6 +585,12 @@ __device__ __forceinline__ void pass_body(const PassParams &p, uint32_t bx, uint
         uint64_t off;
         tile_elem<K, C>(e, g, off, tg.base_off, p.lb);
         const uint32_t col = c0 + g;
+        if (col < tg.col_end && async_copy) {
+          const uint64_t *src = in + (uint64_t)col * p.stride_in + off;
+          cp_async8(tile + pad16(e), src);
+          cp_async8(tile + pad16(e) + 1, src + 1);
+          continue;
+        }
         uint64_t v0 = 0, v1 = 0;
         if (col < tg.col_end) {
           const uint64_t *src = in + (uint64_t)col * p.stride_in + off;
@@ -575,17 +602,18 @@ __device__ __forceinline__ void pass_body(const PassParams &p, uint32_t bx, uint
             v0 = __ldcg(src);
             v1 = __ldcg(src + 1);
           }
-          if (p.load_scale) {
-            const uint32_t i0 = (uint32_t)off, i1 = (uint32_t)off + 1;
-            const uint32_t n0 = B2N ? brev_bits(i0, p.log_n) : i0;
-            const uint32_t n1 = B2N ? brev_bits(i1 & mask_n, p.log_n) : i1;
-            v0 = gl::mul(v0, coset_power(p.tabs, 0, n0, p.coset_kshift));
-            v1 = gl::mul(v1, coset_power(p.tabs, 0, n1, p.coset_kshift));
-          }
+          const uint32_t i0 = (uint32_t)off, i1 = (uint32_t)off + 1; // load_scale
+          const uint32_t n0 = B2N ? brev_bits(i0, p.log_n) : i0;
+          const uint32_t n1 = B2N ? brev_bits(i1 & mask_n, p.log_n) : i1;
+          v0 = gl::mul(v0, coset_power(p.tabs, 0, n0, p.coset_kshift));
+          v1 = gl::mul(v1, coset_power(p.tabs, 0, n1, p.coset_kshift));
         }
         tile[pad16(e)] = v0;
         tile[pad16(e) + 1] = v1;
       }
+      cp_async_commit();
+      if (c0 == tg.col_begin) fill_powers<K>(pw, p.tabs, INV, Hbig, tid, T);
+      cp_async_wait<0>();
       __syncthreads();
       if constexpr (!B2N) {
         rounds_from<K, C, false, INV, false, 0>(tile, pw, tid, T); // K < 4: one short round
