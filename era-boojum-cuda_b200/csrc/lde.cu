@@ -39,6 +39,22 @@ __global__ void __launch_bounds__(256, BC_TOP_MIN_BLOCKS) lde_top_kernel(const L
 typedef void (*TopKernel)(const LdeTopParams);
 typedef void (*PassKernelT)(const PassParams);
 
+static TopKernel pick_top(int K, int C);
+
+// resident CTAs per SM of lde_top_kernel<K, C> at this block size and dynamic
+// shared memory (0 when the kernel or the query is unavailable)
+static int top_ctas_per_sm(int K, int C, uint32_t threads, size_t smem) {
+  TopKernel kern = pick_top(K, C);
+  if (!kern) return 0;
+  if (smem > 48 * 1024 &&
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TOP_RESIDENT_SMEM_MAX) !=
+          cudaSuccess)
+    return 0;
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, (int)threads, smem) != cudaSuccess) return 0;
+  return n;
+}
+
 template <int K, int C> static TopKernel tk() { return lde_top_kernel<K, C>; }
 
 static TopKernel pick_top(int K, int C) {
@@ -181,7 +197,19 @@ bool build_lde_steps(const Plan &pl, const uint64_t *in, uint64_t *out, uint32_t
     } else {
       p.fwd_mode = TOP_TABLES_REFILL;
     }
-    st.smem = (size_t)top_smem_words(tile, K, slots) * sizeof(uint64_t);
+    // two tiles (the next column group copied during this one) in the 8-column
+    // kernels with short transforms per tile (window bits x cosets <= 16: on
+    // B200 2^16 x 4096 columns, blowup 2, gains 13 %; 2^19 x 512, blowup 4,
+    // loses 2 %), when they fit and cost no resident CTA per SM
+    const size_t smem1 = (size_t)top_smem_words(tile, K, slots, 1) * sizeof(uint64_t);
+    const size_t smem2 = (size_t)top_smem_words(tile, K, slots, 2) * sizeof(uint64_t);
+    p.dbuf = 0;
+    if (C == 8 && (uint32_t)K * nb <= 16 && p.fwd_mode != TOP_TABLES_PREFETCH && p.cols_per_cta > G &&
+        smem2 <= TOP_RESIDENT_SMEM_MAX) {
+      const int n2 = top_ctas_per_sm(K, C, st.threads, smem2);
+      p.dbuf = (n2 > 0 && n2 >= top_ctas_per_sm(K, C, st.threads, smem1)) ? 1 : 0;
+    }
+    st.smem = p.dbuf ? smem2 : smem1;
     const uint64_t gy = (num_cols + p.cols_per_cta - 1) / p.cols_per_cta;
     if (gy > 65535 || tiles > 0x7fffffffull) return false;
     st.grid = dim3((uint32_t)tiles, (uint32_t)gy);

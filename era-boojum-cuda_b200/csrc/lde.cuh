@@ -15,9 +15,11 @@ namespace bc {
 
 enum : uint32_t { TOP_TABLES_REFILL = 0, TOP_TABLES_RESIDENT = 1, TOP_TABLES_PREFETCH = 2 };
 
-// Word offset of the power tables after a padded tile, rounded up to an even
-// word so that 16-byte copies into them are aligned.
-__host__ __device__ constexpr uint32_t top_tables_offset(uint32_t tile) { return (tile + tile / 16 + 1) & ~1u; }
+// Word offset of the power tables after `tiles` padded tiles, rounded up to
+// an even word so that 16-byte copies into them are aligned.
+__host__ __device__ constexpr uint32_t top_tables_offset(uint32_t tile, uint32_t tiles) {
+  return (tiles * (tile + tile / 16) + 1) & ~1u;
+}
 
 // Copies a 2^K-word power table (16-byte aligned both sides) into shared memory:
 // plain 16-byte loads, or cp.async (ASYNC: completion by cp_async_wait).
@@ -52,6 +54,7 @@ struct LdeTopParams {
   uint32_t fwd_mode;
   const uint64_t *fwd_tables; // precomputed forward tables of the cosets (or nullptr)
   const uint64_t *inv_table;  // precomputed inverse table (or nullptr)
+  uint32_t dbuf;              // two tiles: the next column group is copied (cp.async) during this one
   DevTables tabs;
 };
 
@@ -93,10 +96,13 @@ __device__ __forceinline__ void top_body(const LdeTopParams &p, uint32_t bx, uin
   const uint32_t G = 1u << p.log_g;
   const uint32_t TILE = G * W * C;
   const uint32_t T = TILE / 16;
-  uint64_t *tile = smem;
+  // two tiles only in the 8-column kernels (short windows, many column groups
+  // per CTA); the wider windows keep one tile and the registers it saves
+  const bool dbuf = C == 8 && p.dbuf;
+  uint64_t *const tiles[2] = {smem, smem + TILE + TILE / 16};
   // power tables (ntt_pass.cuh): the inverse one, then the forward ones of
-  // fwd_mode (see LdeTopParams)
-  uint64_t *pw_inv = smem + top_tables_offset(TILE); // 16-byte aligned: tables are copied 16 bytes at a time
+  // fwd_mode (see LdeTopParams); 16-byte aligned (copied 16 bytes at a time)
+  uint64_t *pw_inv = smem + top_tables_offset(TILE, dbuf ? 2 : 1);
   uint64_t *pw_fwd = pw_inv + PowWords<K>::words;
   constexpr uint32_t PW = PowWords<K>::words;
   const uint32_t tid = threadIdx.x;
@@ -126,14 +132,15 @@ __device__ __forceinline__ void top_body(const LdeTopParams &p, uint32_t bx, uin
 
   const uint64_t inv_n = p.tabs.inv_pow2[p.log_n];
 
-  for (uint32_t c0 = col_begin; c0 < col_end; c0 += G) {
+  // the tile of column group c by loads and stores
+  auto load_tile = [&](uint64_t *dst, uint32_t c) {
 #pragma unroll
     for (int j = 0; j < 8; j++) {
       const uint32_t e = 2 * (tid + T * j);
       uint32_t g;
       uint64_t off;
       tile_elem<K, C>(e, g, off, base_off, p.lb);
-      const uint32_t col = c0 + g;
+      const uint32_t col = c + g;
       uint64_t v0 = 0, v1 = 0;
       if (col < col_end) {
         const uint64_t *src = p.in + (uint64_t)col * p.stride_in + off;
@@ -146,10 +153,49 @@ __device__ __forceinline__ void top_body(const LdeTopParams &p, uint32_t bx, uin
           v1 = __ldcg(src + 1);
         }
       }
-      tile[pad16(e)] = v0;
-      tile[pad16(e) + 1] = v1;
+      dst[pad16(e)] = v0;
+      dst[pad16(e) + 1] = v1;
     }
-    __syncthreads();
+  };
+  // ... or by 8-byte cp.async (padded slots are 8-byte aligned), rolled so
+  // that it holds no addresses across the transform it overlaps
+  auto load_tile_async = [&](uint64_t *dst, uint32_t c) {
+#pragma unroll 1
+    for (int j = 0; j < 8; j++) {
+      const uint32_t e = 2 * (tid + T * j);
+      uint32_t g;
+      uint64_t off;
+      tile_elem<K, C>(e, g, off, base_off, p.lb);
+      const uint32_t col = c + g;
+      if (col < col_end) {
+        const uint64_t *src = p.in + (uint64_t)col * p.stride_in + off;
+        cp_async8(dst + pad16(e), src);
+        cp_async8(dst + pad16(e) + 1, src + 1);
+      } else {
+        dst[pad16(e)] = 0;
+        dst[pad16(e) + 1] = 0;
+      }
+    }
+  };
+  if (dbuf) {
+    load_tile_async(tiles[0], col_begin);
+    cp_async_commit();
+  }
+
+  uint32_t it = 0;
+  for (uint32_t c0 = col_begin; c0 < col_end; c0 += G, it++) {
+    uint64_t *const tile = tiles[dbuf ? (it & 1) : 0];
+    if (dbuf) {
+      cp_async_wait<0>();
+      __syncthreads(); // this group's tile is complete; the other tile is free
+      if (c0 + G < col_end) {
+        load_tile_async(tiles[(it + 1) & 1], c0 + G);
+        cp_async_commit();
+      }
+    } else {
+      load_tile(tile, c0);
+      __syncthreads();
+    }
 
     if constexpr (NF == 0) {
       // window of fewer than 4 bits: one short round each way, in registers
@@ -273,13 +319,13 @@ __device__ __forceinline__ void top_body(const LdeTopParams &p, uint32_t bx, uin
     }
     __syncthreads();
   }
-  if (p.fwd_mode == TOP_TABLES_PREFETCH) cp_async_wait<0>(); // nothing in flight past the body
+  cp_async_wait<0>(); // nothing in flight past the body
 }
 
-// Shared memory (u64 words) of top_body: tile, padding, the inverse power
-// table and fwd_tables forward ones (or slots).
-__host__ __device__ constexpr uint32_t top_smem_words(uint32_t tile, int K, uint32_t fwd_tables) {
-  return top_tables_offset(tile) + (1 + fwd_tables) * (1u << K);
+// Shared memory (u64 words) of top_body: one or two padded tiles, the
+// inverse power table and fwd_tables forward ones (or slots).
+__host__ __device__ constexpr uint32_t top_smem_words(uint32_t tile, int K, uint32_t fwd_tables, uint32_t tiles = 1) {
+  return top_tables_offset(tile, tiles) + (1 + fwd_tables) * (1u << K);
 }
 
 // Largest shared memory of a top-window kernel whose forward tables stay

@@ -6,7 +6,8 @@
 // of consecutive positions each window's tiles span (the tile shape), and so
 // how many stages the fused LDE's top-window kernel carries (the stage fusion:
 // its window is pass 0).  bc_autotune times every candidate on the current
-// device and stores the fastest (near-ties go to the smallest top window);
+// device and stores the fastest (near-ties go to the fewest passes, then the
+// smallest top window);
 // LDE and NTT entry points consult the table and fall back to the built-in
 // plan.  Candidates use only window shapes that
 // every kernel (the persistent batch kernel included) can run.
@@ -147,16 +148,19 @@ extern "C" cudaError_t bc_autotune(uint32_t log_n, uint32_t log_blowup, uint32_t
     timed.emplace_back(pl, ms);
     best_ms = std::min(best_ms, ms);
   }
-  // Near-ties (within 1 %, below the run-to-run spread) go to the smallest top
-  // window: its top-window kernel has more, shorter tiles, which shortens a
-  // job's critical path inside the persistent batch kernel.
+  // Near-ties (within 1 %, below the run-to-run spread) go to the plan with
+  // the fewest passes (one HBM round trip each, which the tuning shape's
+  // column count may hide), then to the smallest top window: its top-window
+  // kernel has more, shorter tiles, which shortens a job's critical path
+  // inside the persistent batch kernel.
   {
     float pick_ms = 1e30f;
-    int pick_k = 1 << 30;
+    int pick_np = 1 << 30, pick_k = 1 << 30;
     for (const auto &c : timed) {
       if (c.second > best_ms * 1.01f) continue;
-      const int k0 = c.first.pass[0].K;
-      if (k0 < pick_k || (k0 == pick_k && c.second < pick_ms)) {
+      const int np = c.first.npasses, k0 = c.first.pass[0].K;
+      if (np < pick_np || (np == pick_np && (k0 < pick_k || (k0 == pick_k && c.second < pick_ms)))) {
+        pick_np = np;
         pick_k = k0;
         pick_ms = c.second;
         best = c.first;

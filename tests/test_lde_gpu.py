@@ -137,6 +137,29 @@ def test_lde_benchmark_size_fused_equals_plain(gpu_ctx):
             np.testing.assert_array_equal(to_host(a[(k * cols + c) * n:(k * cols + c + 1) * n]), exp[k])
 
 
+@pytest.mark.parametrize("log_n,cols,log_b", [(16, 1029, 1), (20, 37, 1), (13, 4099, 1), (14, 2051, 2), (18, 301, 1)])
+def test_lde_many_column_groups_fused_equals_plain(gpu_ctx, log_n, cols, log_b):
+    """Many column groups per top-window CTA (two-tile pipelining in the short windows), ragged last group:
+    fused == plain on the device, first and last columns against the oracle."""
+    import bc_ntt
+    import torch
+
+    n, B = 1 << log_n, 1 << log_b
+    g = torch.Generator(device="cuda").manual_seed(log_n + cols)
+    x = torch.randint(-(2**63), 2**63 - 1, (cols * n,), device="cuda", dtype=torch.int64, generator=g)
+    a = torch.empty(B * cols * n, dtype=torch.int64, device="cuda")
+    bc_ntt.lde(x, a, log_n, cols, log_b, fused=True)
+    b = torch.empty_like(a)
+    bc_ntt.lde(x, b, log_n, cols, log_b, fused=False)
+    torch.cuda.synchronize()
+    assert torch.equal(a, b)
+    for c in (0, cols - 1):
+        xc = to_host(x[c * n:(c + 1) * n])
+        exp = oracle.lde(xc, log_n, 1, n, log_b, threads=2).reshape(B, n)
+        for k in range(B):
+            np.testing.assert_array_equal(to_host(a[(k * cols + c) * n:(k * cols + c + 1) * n]), exp[k])
+
+
 @pytest.mark.parametrize("pinned", [False, True])
 def test_lde_host_pipeline_matches_device(gpu_ctx, pinned):
     """bc_lde_host (host in, host out, chunked through a device workspace) == bc_lde_fused on the device."""
