@@ -35,6 +35,7 @@ sys.path.insert(0, os.path.join(ROOT, "era-boojum-cuda_b200"))
 P = 0xFFFFFFFF00000001
 METRIC = "bit-exact Goldilocks LDE Melem/s: batched vs plain, % HBM roofline; p99 ms"
 LOG_N, COLS, LOG_BLOWUP = 22, 128, 1
+SPEC_HBM_GBS = 8000.0  # B200 HBM3e specification (DGX figure), for the spec fraction beside the measured one
 
 
 def measured_peaks():
@@ -218,9 +219,78 @@ def cpu_baseline(threads: int, budget_s: float = 12.0):
         oracle.lde(x, LOG_N, cols, n, LOG_BLOWUP, threads=threads)
     dt = (time.perf_counter() - t0) / reps
     out_elems = (1 << LOG_BLOWUP) * n * cols
+    model = "unknown"
+    try:
+        with open("/proc/cpuinfo") as f:
+            model = next((ln.split(":", 1)[1].strip() for ln in f if ln.startswith("model name")), model)
+    except OSError:
+        pass
     return {"value": out_elems / dt / 1e6, "unit": "Melem/s", "cores": threads, "kind": "port",
+            "nproc": os.cpu_count(), "cpu_model": model,
             "sample": f"{cols} of {COLS} columns (2^{LOG_N}, blowup {1 << LOG_BLOWUP}) x {reps} reps, "
                       f"{dt:.2f} s each; oracle/gl_oracle.c, one column per thread"}
+
+
+def run_small_ntt_section(call, reps: int = 200, log_n: int = 16, cols: int = 16):
+    """Plain forward NTT (natural in, bit-reversed out, no coset) of 16 columns x 2^16: a latency-bound call.
+    Device time of each call (CUDA events around it) over `reps` calls, and `reps` calls issued back to back
+    under one event pair; `call(in_ptr, out_ptr, log_n, cols, stream)`.  The 8 MiB of columns stay in L2, as
+    they do for a caller that issues this call repeatedly."""
+    import torch
+
+    n = 1 << log_n
+    stream = torch.cuda.current_stream()
+    g = torch.Generator(device="cuda").manual_seed(16)
+    x = torch.randint(0, 2**62, (cols * n,), dtype=torch.int64, device="cuda", generator=g)
+    y = torch.empty_like(x)
+    for _ in range(20):
+        call(x.data_ptr(), y.data_ptr(), log_n, cols, stream.cuda_stream)
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+    for a, b in evs:
+        a.record(stream)
+        call(x.data_ptr(), y.data_ptr(), log_n, cols, stream.cuda_stream)
+        b.record(stream)
+        torch.cuda.synchronize()
+    per_us = [a.elapsed_time(b) * 1e3 for a, b in evs]
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(reps):
+        call(x.data_ptr(), y.data_ptr(), log_n, cols, stream.cuda_stream)
+    b.record(stream)
+    torch.cuda.synchronize()
+    b2b_us = a.elapsed_time(b) * 1e3 / reps
+    del x, y
+    return {"workload": f"forward NTT {cols} cols x 2^{log_n}, natural -> bit-reversed", "reps": reps,
+            "p50_us": round(pct(per_us, 50), 2), "p99_us": round(pct(per_us, 99), 2),
+            "back_to_back_us": round(b2b_us, 2), "melem_per_s": round(cols * n / b2b_us, 1),
+            "l2": "8 MiB of columns, L2-resident across calls"}
+
+
+def copy_floor_ms(h_in, d_in, d_out, h_out, stream, reps: int = 3) -> float:
+    """The e2e leg's host<->device copies alone: the whole input host->device and the whole output
+    device->host, issued at once on two streams (full-duplex PCIe), no transform; the best of `reps`."""
+    import torch
+
+    s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    best = None
+    for i in range(reps + 1):
+        torch.cuda.synchronize()
+        a.record(stream)
+        s_in.wait_stream(stream)
+        s_out.wait_stream(stream)
+        with torch.cuda.stream(s_in):
+            d_in.copy_(h_in, non_blocking=True)
+        with torch.cuda.stream(s_out):
+            h_out.copy_(d_out, non_blocking=True)
+        stream.wait_stream(s_in)
+        stream.wait_stream(s_out)
+        b.record(stream)
+        torch.cuda.synchronize()
+        if i > 0:
+            best = a.elapsed_time(b) if best is None else min(best, a.elapsed_time(b))
+    return best
 
 
 def run_ours(args, rank, world):
@@ -304,6 +374,7 @@ def run_ours(args, rank, world):
         achieved = byts / (kern_ms[dom] / 1e3) / 1e9
         roofline = {"bound": "hbm", "kernel": name, "achieved": round(achieved, 1), "peak": peak,
                     "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+                    "spec_frac": round(achieved / SPEC_HBM_GBS, 4),
                     "traffic": traffic if "lde_top_kernel" in name else None,
                     "traffic_unit": "bytes per launch (ncu dram read+write, scaled from the profiled case)",
                     "kernel_ms": [round(v, 3) for v in kern_ms],
@@ -329,6 +400,7 @@ def run_ours(args, rank, world):
     fused()
     torch.cuda.synchronize()
     e2e_exact = bool(torch.equal(hout, out.cpu())) if COLS * n <= (1 << 30) else None
+    floor_ms = copy_floor_ms(hx, x, out, hout, stream)
 
     line = {
         "metric": METRIC, "value": round(value, 1), "unit": "Melem/s", "n_gpus": world, "steps": args.steps,
@@ -347,12 +419,20 @@ def run_ours(args, rank, world):
         "e2e": {"value": round(e2e_value, 1), "unit": "Melem/s", "h2d_bytes_per_step": 8 * COLS * n,
                 "d2h_bytes_per_step": 8 * B * COLS * n, "ms_per_step": round(e2e_ms / e2e_steps, 3),
                 "path": f"bc_lde_host: pinned host in/out, {chunk_cols}-column chunks, copies overlapped",
-                "bit_exact_vs_device": e2e_exact},
+                "bit_exact_vs_device": e2e_exact, "copy_floor_ms": round(floor_ms, 3),
+                "frac_of_copy_floor": round(floor_ms / (e2e_ms / e2e_steps), 4)},
         "gpu_launches": args.steps * (len(kern_ms) if kern_ms else 3),
     }
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(os.cpu_count() or 1)
     del x, out, hx, hout, ws
+    torch.cuda.empty_cache()
+    if world == 1:
+        def small_call(a, b, log_n, cols, s):
+            rc = L.bc_batch_ntt_internal(a, b, log_n, cols, 1 << log_n, 1 << log_n, False, False, 0, 0, s)
+            assert rc == 0, rc
+
+        line["small_ntt"] = run_small_ntt_section(small_call)
     torch.cuda.empty_cache()
     if world == 1 and not args.no_batch:
         line["batch"] = run_batch_section()
@@ -743,6 +823,9 @@ def run_reference(args, rank, world):
     e2e_ms, _ = time_steps(e2e_step, e2e_steps, 1, world, stream)
     del dx, hx, hout, x, out, coef
     torch.cuda.empty_cache()
+    small = run_small_ntt_section(
+        lambda a, b, log_n, cols, s: ref.batch_ntt(a, b, log_n, cols, 1 << log_n, 1 << log_n, False, False, 0, 0, s)) \
+        if world == 1 else None
     ops = run_ops_section(ops_reference(ref), log_n=args.ops_log_n,
                           note="batch_eval_*: the reference's partial-reduce kernel only; "
                           "the CUB column sums that its Rust side runs after it are not timed") \
@@ -762,6 +845,8 @@ def run_reference(args, rank, world):
                 "h2d_bytes_per_step": 8 * COLS * n, "d2h_bytes_per_step": 8 * B * COLS * n,
                 "ms_per_step": round(e2e_ms / e2e_steps, 3)},
     }
+    if small is not None:
+        line["small_ntt"] = small
     if ops is not None:
         line["ops"] = ops
     return line

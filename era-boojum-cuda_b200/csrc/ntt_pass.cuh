@@ -536,6 +536,32 @@ __device__ __forceinline__ void pass_body(const PassParams &p, uint32_t bx, uint
     col = c0 + g;
   };
 
+  // 8-byte cp.async copy of column group c's tile (padded slots are only
+  // 8-byte aligned); slots of columns past the chunk are zeroed
+  auto copy_tile_async = [&](uint32_t c) {
+#pragma unroll 1
+    for (int j = 0; j < 8; j++) {
+      const uint32_t e = 2 * (tid + T * j);
+      uint32_t g;
+      uint64_t off;
+      tile_elem<K, C>(e, g, off, tg.base_off, p.lb);
+      const uint32_t col = c + g;
+      if (col < tg.col_end) {
+        const uint64_t *src = in + (uint64_t)col * p.stride_in + off;
+        cp_async8(tile + pad16(e), src);
+        cp_async8(tile + pad16(e) + 1, src + 1);
+      } else {
+        tile[pad16(e)] = 0;
+        tile[pad16(e) + 1] = 0;
+      }
+    }
+    cp_async_commit();
+  };
+  // bit-reversed -> natural with a plain copy: the last round has the whole
+  // tile in registers, so the next group's copy is issued into the tile then
+  // and overlaps that round's arithmetic and stores
+  bool prefetched = false;
+
   for (uint32_t c0 = tg.col_begin; c0 < tg.col_end; c0 += G) {
     if constexpr (!B2N && NF > 0) {
       __syncthreads(); // powers ready; previous column group's stores done
@@ -579,7 +605,7 @@ __device__ __forceinline__ void pass_body(const PassParams &p, uint32_t bx, uint
       // 8-byte aligned), completed after the first group's table fill
       const bool async_copy = !p.load_scale;
 #pragma unroll
-      for (int j = 0; j < 8; j++) {
+      for (int j = 0; j < 8 && !prefetched; j++) {
         const uint32_t e = 2 * (tid + T * j);
         uint32_t g;
         uint64_t off;
@@ -631,6 +657,11 @@ __device__ __forceinline__ void pass_body(const PassParams &p, uint32_t bx, uint
         uint64_t x[16];
 #pragma unroll
         for (int j = 0; j < 16; j++) x[j] = tile[a[j]];
+        prefetched = async_copy && c0 + G < tg.col_end;
+        if (prefetched) {
+          __syncthreads(); // every thread holds its values: the tile is free
+          copy_tile_async(c0 + G);
+        }
         net16<K, true, INV>(x, pw, w, B, top_s && !p.store_scale);
         uint64_t off0;
         uint32_t col;
@@ -654,7 +685,7 @@ __device__ __forceinline__ void pass_body(const PassParams &p, uint32_t bx, uint
 #pragma unroll
           for (int j = 0; j < 16; j++) __stcg(dst + j * step, p.canon_out ? gl::canon(x[j]) : x[j]);
         }
-        __syncthreads();
+        if (!prefetched) __syncthreads();
         continue;
       }
     }
