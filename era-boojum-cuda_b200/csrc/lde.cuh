@@ -87,6 +87,35 @@ __device__ __forceinline__ void top_store_t(const LdeTopParams &p, const uint64_
 }
 #define top_store top_store_t<K, C>
 
+// top_store_t from the values v[2j], v[2j + 1] of tile elements 2 (tid + T j), + 1.
+template <int K, int C>
+__device__ __forceinline__ void top_store_regs(const LdeTopParams &p, const uint64_t (&v)[16], uint32_t c0,
+                                               uint32_t col_end, uint32_t k, uint64_t base_off, uint32_t tid,
+                                               uint32_t T) {
+  uint64_t *out = p.out + (uint64_t)k * p.coset_stride;
+#pragma unroll
+  for (int j = 0; j < 8; j++) {
+    const uint32_t e = 2 * (tid + T * j);
+    uint32_t g;
+    uint64_t off;
+    tile_elem<K, C>(e, g, off, base_off, p.lb);
+    const uint32_t col = c0 + g;
+    if (col >= col_end) continue;
+    uint64_t v0 = v[2 * j], v1 = v[2 * j + 1];
+    if (p.canon_out) {
+      v0 = gl::canon(v0);
+      v1 = gl::canon(v1);
+    }
+    uint64_t *dst = out + (uint64_t)col * p.stride_out + off;
+    if (p.vec_out) {
+      *reinterpret_cast<ulonglong2 *>(dst) = make_ulonglong2(v0, v1);
+    } else {
+      dst[0] = v0;
+      dst[1] = v1;
+    }
+  }
+}
+
 // One CTA's work of the top-window kernel: tile position bx (run of low
 // positions), column chunk by.  blockDim.x == 2^log_g * 2^K * C / 16.
 template <int K, int C>
@@ -182,6 +211,7 @@ __device__ __forceinline__ void top_body(const LdeTopParams &p, uint32_t bx, uin
     cp_async_commit();
   }
 
+  bool prefetched = false; // this group's tile was copied during the previous group
   uint32_t it = 0;
   for (uint32_t c0 = col_begin; c0 < col_end; c0 += G, it++) {
     uint64_t *const tile = tiles[dbuf ? (it & 1) : 0];
@@ -192,10 +222,14 @@ __device__ __forceinline__ void top_body(const LdeTopParams &p, uint32_t bx, uin
         load_tile_async(tiles[(it + 1) & 1], c0 + G);
         cp_async_commit();
       }
+    } else if (prefetched) {
+      cp_async_wait<0>(); // copied during the previous group's last store
+      __syncthreads();
     } else {
       load_tile(tile, c0);
       __syncthreads();
     }
+    prefetched = false;
 
     if constexpr (NF == 0) {
       // window of fewer than 4 bits: one short round each way, in registers
@@ -314,10 +348,29 @@ __device__ __forceinline__ void top_body(const LdeTopParams &p, uint32_t bx, uin
           __syncthreads();
         }
         if constexpr (R > 0) rounds_from<K, C, false, false, false, NF>(tile, pwk, tid, T);
-        top_store(p, tile, c0, col_end, k, base_off, tid, T);
+        if (k + 1 == nb && !dbuf && p.fwd_mode != TOP_TABLES_PREFETCH && c0 + G < col_end) {
+          // last coset: the values go to registers, then the next group's tile
+          // is copied into the tile while they are stored (not with prefetched
+          // tables, whose next copy the tile's wait would then also wait for:
+          // 2^23 x 64 columns, blowup 4 measured 2.4 % slower)
+          uint64_t v[16];
+#pragma unroll
+          for (int j = 0; j < 8; j++) {
+            const uint32_t e = 2 * (tid + T * j);
+            v[2 * j] = tile[pad16(e)];
+            v[2 * j + 1] = tile[pad16(e) + 1];
+          }
+          __syncthreads();
+          load_tile_async(tile, c0 + G);
+          cp_async_commit();
+          prefetched = true;
+          top_store_regs<K, C>(p, v, c0, col_end, k, base_off, tid, T);
+        } else {
+          top_store(p, tile, c0, col_end, k, base_off, tid, T);
+        }
       }
     }
-    __syncthreads();
+    if (!prefetched) __syncthreads(); // the tile is read; a prefetch already waited for that
   }
   cp_async_wait<0>(); // nothing in flight past the body
 }
