@@ -35,6 +35,7 @@ sys.path.insert(0, os.path.join(ROOT, "era-boojum-cuda_b200"))
 P = 0xFFFFFFFF00000001
 METRIC = "bit-exact Goldilocks LDE Melem/s: batched vs plain, % HBM roofline; p99 ms"
 LOG_N, COLS, LOG_BLOWUP = 22, 128, 1
+L2_BYTES = 126 * 2**20  # B200 L2
 SPEC_HBM_GBS = 8000.0  # B200 HBM3e specification (DGX figure), for the spec fraction beside the measured one
 
 
@@ -45,6 +46,16 @@ def measured_peaks():
         return float(d["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
+
+
+def l2_note() -> str:
+    """How the timed LDE relates to the 126 MB L2 (inputs and outputs of the configured workload)."""
+    n_in = 8 * COLS * (1 << LOG_N)
+    n_out = n_in << LOG_BLOWUP
+    fmt = lambda b: f"{b / 2**30:g} GiB" if b >= 2**30 else f"{b / 2**20:g} MiB"  # noqa: E731
+    if n_in > L2_BYTES:
+        return f"inputs {fmt(n_in)} and outputs {fmt(n_out)}, larger than L2; no flush"
+    return f"inputs {fmt(n_in)} and outputs {fmt(n_out)}; inputs fit in L2 (a small case, not the bench workload)"
 
 
 def measured_traffic(log_n: int, log_blowup: int, cols: int):
@@ -409,7 +420,7 @@ def run_ours(args, rank, world):
         "config": {"workload": f"coset LDE {COLS} cols x 2^{LOG_N}, blowup {B}, bit-reversed in/out",
                    "log_n": LOG_N, "columns": COLS, "blowup": B, "path": "bc_lde_fused",
                    "plans": "autotuned (era-boojum-cuda_b200/plans_b200.txt)" if tuned else "built-in",
-                   "l2": "inputs 4 GiB and outputs 8 GiB, larger than L2; no flush", "parallelism": f"replicas x{world}"},
+                   "l2": l2_note(), "parallelism": f"replicas x{world}"},
         "p50_ms": round(pct(per, 50), 4), "p99_ms": round(pct(per, 99), 4),
         "plain": {"value": round(world * len(plain_per) * out_elems / (plain_ms / 1e3) / 1e6, 1),
                   "ms_per_step": round(plain_ms / len(plain_per), 4), "path": "bc_lde_plain",
@@ -839,7 +850,7 @@ def run_reference(args, rank, world):
                            "has no CPU implementation of this path (boojum's CPU NTT is not vendored)"),
         "config": {"workload": f"coset LDE {COLS} cols x 2^{LOG_N}, blowup {B}, bit-reversed in/out",
                    "log_n": LOG_N, "columns": COLS, "blowup": B, "path": "reference kernels",
-                   "l2": "inputs 4 GiB and outputs 8 GiB, larger than L2; no flush", "parallelism": f"replicas x{world}"},
+                   "l2": l2_note(), "parallelism": f"replicas x{world}"},
         "p50_ms": round(pct(per, 50), 4), "p99_ms": round(pct(per, 99), 4), "clocks": clk.summary(),
         "e2e": {"value": round(world * e2e_steps * out_elems / (e2e_ms / 1e3) / 1e6, 1), "unit": "Melem/s",
                 "h2d_bytes_per_step": 8 * COLS * n, "d2h_bytes_per_step": 8 * B * COLS * n,
