@@ -59,17 +59,20 @@ def l2_note() -> str:
 
 
 def measured_traffic(log_n: int, log_blowup: int, cols: int):
-    """DRAM bytes of one top-window launch from the committed ncu summary, scaled to `cols` columns."""
+    """DRAM bytes of one top-window launch from the committed ncu summary, scaled to `cols` columns, and the
+    ALU / FMA pipe utilisation (% of peak) of that capture: (bytes, alu_pct, fma_pct), Nones if absent."""
     path = os.path.join(ROOT, "profiles", f"lde_top_kernel_traffic_logn{log_n}_blowup{1 << log_blowup}.txt")
     try:
         for line in open(path):
             if line.startswith("kernel="):
                 kv = dict(tok.split("=", 1) for tok in line.split())
                 if int(kv["log_n"]) == log_n and int(kv["log_blowup"]) == log_blowup:
-                    return round((int(kv["dram_read"]) + int(kv["dram_write"])) * cols / int(kv["cols"]))
+                    byts = round((int(kv["dram_read"]) + int(kv["dram_write"])) * cols / int(kv["cols"]))
+                    alu, fma = kv.get("alu_pipe_pct"), kv.get("fma_pipe_pct")
+                    return byts, float(alu) if alu else None, float(fma) if fma else None
     except OSError:
         pass
-    return None
+    return None, None, None
 
 
 class ClockSampler:
@@ -378,18 +381,23 @@ def run_ours(args, rank, world):
                    (1 + B) * col_bytes)]
                + [(f"lde forward pass {i} (n2b, all cosets)", 2 * B * col_bytes) for i in range(npass - 1)])
     roofline = None
-    traffic = measured_traffic(LOG_N, LOG_BLOWUP, COLS)
+    traffic, alu_pct, fma_pct = measured_traffic(LOG_N, LOG_BLOWUP, COLS)
     if kern_ms and len(kern_ms) == len(kernels):
         dom = max(range(len(kern_ms)), key=lambda i: kern_ms[i])
         name, byts = kernels[dom]
         achieved = byts / (kern_ms[dom] / 1e3) / 1e9
+        top = "lde_top_kernel" in name
         roofline = {"bound": "hbm", "kernel": name, "achieved": round(achieved, 1), "peak": peak,
                     "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
                     "spec_frac": round(achieved / SPEC_HBM_GBS, 4),
-                    "traffic": traffic if "lde_top_kernel" in name else None,
+                    "traffic": traffic if top else None,
                     "traffic_unit": "bytes per launch (ncu dram read+write, scaled from the profiled case)",
                     "kernel_ms": [round(v, 3) for v in kern_ms],
                     "step_algorithmic_frac": round(8 * n * COLS * (1 + B) / (ms_per_step / 1e3) / 1e9 / peak, 4)}
+        if top and alu_pct is not None:
+            # what bounds the kernel instead of HBM: 32-bit integer issue (ncu capture of the same kernel)
+            roofline["limiter"] = {"kind": "int32 issue", "alu_pipe_pct": alu_pct, "fma_pipe_pct": fma_pct,
+                                   "source": "ncu --set full, profiles/lde_kernels_ncu_full_8cols_logn22_blowup2.md"}
 
     # end to end through the C ABI with host buffers: bc_lde_host takes pinned host input and writes pinned
     # host output every step, overlapping chunked copy-in / transform / copy-out on three streams
