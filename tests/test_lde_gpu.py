@@ -137,10 +137,12 @@ def test_lde_benchmark_size_fused_equals_plain(gpu_ctx):
             np.testing.assert_array_equal(to_host(a[(k * cols + c) * n:(k * cols + c + 1) * n]), exp[k])
 
 
-@pytest.mark.parametrize("log_n,cols,log_b", [(16, 1029, 1), (20, 37, 1), (13, 4099, 1), (14, 2051, 2), (18, 301, 1)])
+@pytest.mark.parametrize("log_n,cols,log_b", [(16, 1029, 1), (20, 37, 1), (13, 4099, 1), (14, 2051, 2), (18, 301, 1),
+                                              (21, 100, 1), (19, 203, 2)])
 def test_lde_many_column_groups_fused_equals_plain(gpu_ctx, log_n, cols, log_b):
-    """Many column groups per top-window CTA (two-tile pipelining in the short windows), ragged last group:
-    fused == plain on the device, first and last columns against the oracle."""
+    """Many column groups per top-window CTA, ragged last group: two-tile pipelining in the short windows
+    (the first five shapes), the next tile copied during the last coset's stores (the last two).  Fused ==
+    plain on the device, first and last columns against the oracle."""
     import bc_ntt
     import torch
 
