@@ -24,6 +24,9 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <map>
+#include <mutex>
+#include <tuple>
 
 #include "../../include/bc_ntt.h"
 #include "lde.cuh"
@@ -42,8 +45,19 @@ typedef void (*PassKernelT)(const PassParams);
 static TopKernel pick_top(int K, int C);
 
 // resident CTAs per SM of lde_top_kernel<K, C> at this block size and dynamic
-// shared memory (0 when the kernel or the query is unavailable)
+// shared memory (0 when the kernel or the query is unavailable); cached per
+// device and shape, since every fused-LDE call that may pipeline asks
 static int top_ctas_per_sm(int K, int C, uint32_t threads, size_t smem) {
+  static std::mutex mu;
+  static std::map<std::tuple<int, int, int, uint32_t, size_t>, int> cache;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  const auto key = std::make_tuple(dev, K, C, threads, smem);
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    const auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+  }
   TopKernel kern = pick_top(K, C);
   if (!kern) return 0;
   if (smem > 48 * 1024 &&
@@ -52,6 +66,8 @@ static int top_ctas_per_sm(int K, int C, uint32_t threads, size_t smem) {
     return 0;
   int n = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, (int)threads, smem) != cudaSuccess) return 0;
+  std::lock_guard<std::mutex> lock(mu);
+  cache[key] = n;
   return n;
 }
 
