@@ -188,6 +188,7 @@ bool build_lde_steps(const Plan &pl, const uint64_t *in, uint64_t *out, uint32_t
     uint64_t factor = (tiles * chunks) / ((uint64_t)sm_count() * 8);
     if (factor < 1) factor = 1;
     if (factor > (uint64_t)cols_factor_max) factor = cols_factor_max;
+    if (factor > (uint64_t)BC_TOP_COLS_FACTOR_MAX) factor = BC_TOP_COLS_FACTOR_MAX;
     p.cols_per_cta = G * (uint32_t)factor;
     p.canon_out = np == 1;
     p.vec_in = ((uintptr_t)p.in % 16 == 0 && p.stride_in % 2 == 0) ? 1 : 0;
@@ -286,8 +287,8 @@ cudaError_t lde_fused(const Plan &pl, const uint64_t *in, uint64_t *out, uint32_
   if (!device_tables()) return cudaErrorInitializationError;
   if (num_cols == 0) return cudaSuccess;
   std::vector<LdeStep> steps;
-  if (!build_lde_steps(pl, in, out, log_n, num_cols, stride_in, stride_out, coset_stride, log_blowup, false, 8,
-                       steps))
+  if (!build_lde_steps(pl, in, out, log_n, num_cols, stride_in, stride_out, coset_stride, log_blowup, false,
+                       BC_COLS_FACTOR_MAX, steps))
     return cudaErrorInvalidConfiguration;
   uint32_t ev_used = 0;
   if (ev_used < n_ev) cudaEventRecord(ev[ev_used++], stream);

@@ -401,7 +401,7 @@ cudaError_t launch_pass(const PassLaunch &pl, cudaStream_t stream) {
   dim3 grid;
   uint32_t threads;
   size_t smem;
-  if (!build_pass(pl, 8, p, grid, threads, smem)) return cudaErrorInvalidConfiguration;
+  if (!build_pass(pl, BC_COLS_FACTOR_MAX, p, grid, threads, smem)) return cudaErrorInvalidConfiguration;
   PassKernel kern = pick_pass_kernel(pl.K, pl.C, pl.b2n, pl.inverse);
   if (!kern) return cudaErrorInvalidValue;
   if (smem > 48 * 1024) {

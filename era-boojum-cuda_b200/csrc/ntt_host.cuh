@@ -60,6 +60,17 @@ struct PassLaunch {
 cudaError_t launch_pass(const PassLaunch &pl, cudaStream_t stream);
 
 struct PassParams;
+// Column groups one standalone pass CTA walks at most (it fills its power
+// table once per walk; the walk is shortened to keep >= 8 CTAs per SM).  On
+// B200, 16 against 8: forward 12-bit passes 1.8 % faster, 32 no better.  The
+// top-window kernel, which copies precomputed tables, walks at most
+// BC_TOP_COLS_FACTOR_MAX (16 was 0.5-4 % slower there).
+#ifndef BC_COLS_FACTOR_MAX
+#define BC_COLS_FACTOR_MAX 16
+#endif
+#ifndef BC_TOP_COLS_FACTOR_MAX
+#define BC_TOP_COLS_FACTOR_MAX 8
+#endif
 // Kernel parameters, grid, block size and shared memory of one pass (no launch).
 // cols_factor_max bounds how many column groups one CTA walks.
 bool build_pass(const PassLaunch &pl, int cols_factor_max, PassParams &p, dim3 &grid, uint32_t &threads,
