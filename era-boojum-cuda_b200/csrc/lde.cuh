@@ -54,7 +54,8 @@ struct LdeTopParams {
   uint32_t fwd_mode;
   const uint64_t *fwd_tables; // precomputed forward tables of the cosets (or nullptr)
   const uint64_t *inv_table;  // precomputed inverse table (or nullptr)
-  uint32_t dbuf;              // two tiles: the next column group is copied (cp.async) during this one
+  uint32_t dbuf;              // two tiles, the next column group copied (cp.async) during this one;
+                              // honoured by the 8-column kernels only (C == 8)
   DevTables tabs;
 };
 
