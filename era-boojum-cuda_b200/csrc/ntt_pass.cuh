@@ -12,8 +12,12 @@
 // r = idx >> (a + 1) uses twiddle T[r] (see tables.cuh); T[r] does not depend
 // on the stage, exactly as in the reference (native/ntt.cu:23-35).
 //
-// Tile loads bypass L1 (ld.global.cg): a tile is read once, and in the
-// persistent batch kernel another SM may have written it during this launch.
+// Plain tile loads bypass L1 (ld.global.cg): a tile is read once.  The 8-byte
+// cp.async tile copies can only be .ca (the padded slots are not 16-byte
+// aligned); in the persistent batch kernel, where another SM may have written
+// a tile during the launch, a CTA reads a job's tiles only after an
+// ld.acquire.gpu of the producing kernel's counter and a barrier, which
+// orders those reads after the writes in the PTX memory model.
 //
 // Tile.  A CTA owns one tile position: the bits above the window (H) and a
 // run of C consecutive values of the bits below it (l0 .. l0 + C - 1), and
