@@ -71,6 +71,7 @@ SIGNATURES = {
     "bc_lde_server_poll": [_vp, _u64, _vp, _vp],
     "bc_lde_server_wait": [_vp, _u64, _u32, _vp],
     "bc_lde_server_cancel": [_vp, _u64],
+    "bc_lde_server_release": [_vp, _u64],
     "bc_lde_server_get_stats": [_vp, _vp],
     "bc_lde_server_destroy": [_vp],
     "bc_bit_reverse": [_vp, _u64, _vp, _u64, _u32, _u32, _vp],
@@ -316,6 +317,16 @@ class LdeServer:
         if rc == CUDA_ERROR_NOT_READY:
             return False
         _check(rc, "bc_lde_server_cancel")
+        return True
+
+    def release(self, rid: int) -> bool:
+        """Forgets a finished (done, cancelled or failed) request and drops the host buffers kept for it;
+        False while it is pending or running."""
+        rc = lib().bc_lde_server_release(self.handle, rid)
+        if rc == CUDA_ERROR_NOT_READY:
+            return False
+        _check(rc, "bc_lde_server_release")
+        self._keep.pop(rid, None)
         return True
 
     def stats(self) -> dict:

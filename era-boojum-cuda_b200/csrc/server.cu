@@ -104,6 +104,7 @@ struct bc_lde_server {
   Arena arena;
   std::vector<HostPipe> pipes;
   std::vector<int> slot_busy;
+  std::vector<Request *> slot_req; // the request holding each slot (until retired)
   std::mutex mu;
   std::condition_variable cv;      // worker wake-up
   std::condition_variable done_cv; // request completions
@@ -116,7 +117,10 @@ struct bc_lde_server {
   uint64_t completed = 0, out_elems = 0;
   double busy_ms = 0;
   Clock::time_point first_submit{}, last_finish{};
+  // latencies of the last LAT_WINDOW completed requests (ring), the worst of all
   std::vector<double> latencies_ms;
+  size_t lat_next = 0;
+  double max_latency_ms = 0;
 };
 
 namespace {
@@ -138,6 +142,30 @@ void CUDART_CB on_request_done(void *p) {
   d->srv->cv.notify_all();
   d->srv->done_cv.notify_all();
   delete d;
+}
+
+constexpr size_t LAT_WINDOW = 1u << 16;
+
+// Frees a finished request's slot and arena region and books its latency
+// (caller holds the lock; no-op unless the request holds a slot and finished).
+void retire(bc_lde_server *s, Request *r) {
+  if (r->slot < 0 || (r->state != DONE && r->state != FAILED)) return;
+  s->slot_busy[r->slot] = 0;
+  s->slot_req[r->slot] = nullptr;
+  s->arena.release(r->arena_off, r->arena_bytes);
+  r->slot = -1;
+  if (r->state == DONE) {
+    const double lat = std::chrono::duration<double, std::milli>(r->finish - r->submit).count();
+    if (s->latencies_ms.size() < LAT_WINDOW)
+      s->latencies_ms.push_back(lat);
+    else
+      s->latencies_ms[s->lat_next] = lat;
+    s->lat_next = (s->lat_next + 1) % LAT_WINDOW;
+    s->max_latency_ms = std::max(s->max_latency_ms, lat);
+    s->completed++;
+    s->out_elems += ((uint64_t)r->cols << r->log_n) << r->log_blowup;
+    if (r->finish > s->last_finish) s->last_finish = r->finish;
+  }
 }
 
 size_t request_workspace(const bc_lde_server *s, const Request &r, uint32_t &chunk) {
@@ -166,6 +194,7 @@ bool admit_one(bc_lde_server *s, std::unique_lock<std::mutex> &lock) {
   if (chunk == 0 || !s->arena.alloc(bytes, off)) return false; // wait for memory to free up
   s->pending.pop_front();
   s->slot_busy[slot] = 1;
+  s->slot_req[slot] = r;
   r->slot = slot;
   r->arena_off = off;
   r->arena_bytes = bytes;
@@ -176,7 +205,18 @@ bool admit_one(bc_lde_server *s, std::unique_lock<std::mutex> &lock) {
   const uint64_t n = 1ull << r->log_n;
   cudaError_t e = host_lde_enqueue(hp, r->in, r->out, r->log_n, r->cols, n, n, (uint64_t)r->cols * n, r->log_blowup,
                                    s->arena_base + off / 8, chunk, false, nullptr);
-  if (e == cudaSuccess) e = cudaLaunchHostFunc(hp.s_out, on_request_done, new DoneCtx{s, r});
+  if (e == cudaSuccess) {
+    DoneCtx *d = new (std::nothrow) DoneCtx{s, r};
+    e = d ? cudaLaunchHostFunc(hp.s_out, on_request_done, d) : cudaErrorMemoryAllocation;
+    if (e != cudaSuccess) delete d; // never handed to the stream
+  }
+  if (e != cudaSuccess) {
+    // chunks enqueued before the failure may still run on this slot's streams:
+    // wait for them before the slot and its arena region are handed out again
+    cudaStreamSynchronize(hp.s_in);
+    cudaStreamSynchronize(hp.s_comp);
+    cudaStreamSynchronize(hp.s_out);
+  }
   lock.lock();
   if (e != cudaSuccess) {
     r->error = e;
@@ -192,21 +232,8 @@ void worker_main(bc_lde_server *s) {
   std::unique_lock<std::mutex> lock(s->mu);
   while (!s->stop) {
     // retire finished requests: free their slot and memory
-    for (auto &kv : s->all) {
-      Request *r = kv.second;
-      if ((r->state == DONE || r->state == FAILED) && r->slot >= 0) {
-        s->slot_busy[r->slot] = 0;
-        s->arena.release(r->arena_off, r->arena_bytes);
-        r->slot = -1;
-        if (r->state == DONE) {
-          const double lat = std::chrono::duration<double, std::milli>(r->finish - r->submit).count();
-          s->latencies_ms.push_back(lat);
-          s->completed++;
-          s->out_elems += ((uint64_t)r->cols << r->log_n) << r->log_blowup;
-          if (r->finish > s->last_finish) s->last_finish = r->finish;
-        }
-      }
-    }
+    for (Request *r : s->slot_req)
+      if (r) retire(s, r);
     while (admit_one(s, lock)) {
     }
     s->cv.wait_for(lock, std::chrono::milliseconds(5));
@@ -233,6 +260,7 @@ extern "C" cudaError_t bc_lde_server_create(const bc_lde_server_config *cfg, bc_
   s->arena.init(cfg->memory_budget_bytes);
   s->pipes.resize(cfg->slots);
   s->slot_busy.assign(cfg->slots, 0);
+  s->slot_req.assign(cfg->slots, nullptr);
   for (auto &p : s->pipes) {
     if ((e = host_pipe_init(p)) != cudaSuccess) {
       for (auto &q : s->pipes) host_pipe_destroy(q);
@@ -291,12 +319,17 @@ extern "C" cudaError_t bc_lde_server_poll(bc_lde_server *s, uint64_t id, int *st
 extern "C" cudaError_t bc_lde_server_wait(bc_lde_server *s, uint64_t id, uint32_t timeout_ms, double *latency_ms) {
   if (!s) return cudaErrorInvalidValue;
   std::unique_lock<std::mutex> lock(s->mu);
-  auto it = s->all.find(id);
-  if (it == s->all.end()) return cudaErrorInvalidValue;
-  Request *r = it->second;
-  const bool ok = s->done_cv.wait_for(lock, std::chrono::milliseconds(timeout_ms),
-                                      [&] { return r->state == DONE || r->state == FAILED || r->state == CANCELLED; });
+  if (s->all.find(id) == s->all.end()) return cudaErrorInvalidValue;
+  // the record is looked up again after every wake-up: another thread may
+  // release it meanwhile
+  Request *r = nullptr;
+  const bool ok = s->done_cv.wait_for(lock, std::chrono::milliseconds(timeout_ms), [&] {
+    auto it = s->all.find(id);
+    r = it == s->all.end() ? nullptr : it->second;
+    return !r || r->state == DONE || r->state == FAILED || r->state == CANCELLED;
+  });
   if (!ok) return cudaErrorTimeout;
+  if (!r) return cudaErrorInvalidValue;
   if (latency_ms)
     *latency_ms = (r->state == DONE) ? std::chrono::duration<double, std::milli>(r->finish - r->submit).count() : -1.0;
   if (r->state == FAILED) return r->error;
@@ -318,24 +351,37 @@ extern "C" cudaError_t bc_lde_server_cancel(bc_lde_server *s, uint64_t id) {
   return cudaSuccess;
 }
 
+// Forgets a finished, cancelled or failed request (its id is then unknown);
+// cudaErrorNotReady while it is pending or running.
+extern "C" cudaError_t bc_lde_server_release(bc_lde_server *s, uint64_t id) {
+  if (!s) return cudaErrorInvalidValue;
+  std::lock_guard<std::mutex> lock(s->mu);
+  auto it = s->all.find(id);
+  if (it == s->all.end()) return cudaErrorInvalidValue;
+  Request *r = it->second;
+  if (r->state == PENDING || r->state == RUNNING) return cudaErrorNotReady;
+  retire(s, r); // finished but not yet retired by the worker
+  s->all.erase(it);
+  delete r;
+  s->done_cv.notify_all(); // waiters on this id return
+  return cudaSuccess;
+}
+
 extern "C" cudaError_t bc_lde_server_get_stats(bc_lde_server *s, bc_lde_server_stats *st) {
   if (!s || !st) return cudaErrorInvalidValue;
   std::lock_guard<std::mutex> lock(s->mu);
   *st = bc_lde_server_stats{};
   st->completed = s->completed;
-  uint64_t pend = 0, run = 0;
-  for (auto &kv : s->all) {
-    pend += kv.second->state == PENDING;
-    run += kv.second->state == RUNNING;
-  }
-  st->pending = pend;
+  uint64_t run = 0;
+  for (Request *r : s->slot_req) run += r && r->state == RUNNING;
+  st->pending = s->pending.size();
   st->running = run;
   std::vector<double> l = s->latencies_ms;
   std::sort(l.begin(), l.end());
   auto pct = [&](double q) { return l.empty() ? 0.0 : l[std::min(l.size() - 1, (size_t)(q * (l.size() - 1) + 0.5))]; };
   st->p50_ms = pct(0.50);
   st->p99_ms = pct(0.99);
-  st->max_ms = l.empty() ? 0.0 : l.back();
+  st->max_ms = s->max_latency_ms;
   const double span = std::chrono::duration<double>(s->last_finish - s->first_submit).count();
   st->span_s = span > 0 ? span : 0;
   st->out_melem_per_s = span > 0 ? (double)s->out_elems / span / 1e6 : 0;

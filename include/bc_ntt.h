@@ -223,7 +223,8 @@ typedef struct bc_lde_server_config {
 
 typedef struct bc_lde_server_stats {
   uint64_t completed, pending, running;
-  double p50_ms, p99_ms, max_ms; /* latency = completion - submit, completed requests */
+  double p50_ms, p99_ms;         /* latency = completion - submit, last 65536 completed requests */
+  double max_ms;                 /* worst latency of all completed requests */
   double span_s;                 /* first submit to last completion */
   double out_melem_per_s;        /* output elements of completed requests / span */
   size_t arena_largest_free;
@@ -240,6 +241,11 @@ cudaError_t bc_lde_server_poll(bc_lde_server *server, uint64_t request_id, int *
 cudaError_t bc_lde_server_wait(bc_lde_server *server, uint64_t request_id, uint32_t timeout_ms, double *latency_ms);
 /* Cancels a request not yet admitted (cudaErrorNotReady once it runs or ran). */
 cudaError_t bc_lde_server_cancel(bc_lde_server *server, uint64_t request_id);
+/* Forgets a done, cancelled or failed request: its id is unknown afterwards
+ * (poll/wait return cudaErrorInvalidValue); cudaErrorNotReady while it is
+ * pending or running.  A long-running caller releases what it has collected;
+ * unreleased records are freed by destroy. */
+cudaError_t bc_lde_server_release(bc_lde_server *server, uint64_t request_id);
 cudaError_t bc_lde_server_get_stats(bc_lde_server *server, bc_lde_server_stats *stats);
 /* Cancels pending requests, waits for running ones, frees everything. */
 cudaError_t bc_lde_server_destroy(bc_lde_server *server);

@@ -103,4 +103,17 @@ def test_server_cancel_and_timeout_paths(gpu_ctx):
     assert srv.cancel(head) is False  # already ran
     assert bool((tail_out == sentinel).all())  # the cancelled request never wrote its output
     np.testing.assert_array_equal(head_out.numpy().view(np.uint64), _alone(head_x, 20, 64, 1))
+    # released records are forgotten; the slot and the statistics stay right
+    assert srv.release(head) is True and srv.release(tail) is True
+    with pytest.raises(ValueError):
+        srv.poll(head)
+    with pytest.raises(ValueError):
+        srv.release(tail)
+    again_out = torch.zeros(2 * (4 << 16), dtype=torch.int64).pin_memory()
+    again = srv.submit(_pinned(tail_x), again_out, 16, 4, 1)
+    srv.wait(again, timeout_ms=120000)
+    assert srv.release(again) is True  # finished: its slot is retired here if the worker has not yet
+    np.testing.assert_array_equal(again_out.numpy().view(np.uint64), _alone(tail_x, 16, 4, 1))
+    st = srv.stats()
+    assert st["completed"] == 2 and st["pending"] == 0 and st["running"] == 0
     srv.close()
