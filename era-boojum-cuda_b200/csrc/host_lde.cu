@@ -28,28 +28,32 @@ std::mutex g_pipe_mutex[HOST_MAX_DEVICES];
 
 cudaError_t host_pipe_init(HostPipe &hp) {
   if (hp.live) return cudaSuccess;
-  cudaError_t e;
-  if ((e = cudaStreamCreateWithFlags(&hp.s_in, cudaStreamNonBlocking)) != cudaSuccess) return e;
-  if ((e = cudaStreamCreateWithFlags(&hp.s_comp, cudaStreamNonBlocking)) != cudaSuccess) return e;
-  if ((e = cudaStreamCreateWithFlags(&hp.s_out, cudaStreamNonBlocking)) != cudaSuccess) return e;
+  cudaError_t e = cudaSuccess;
+  auto fail = [&]() {
+    host_pipe_destroy(hp); // what was created so far
+    return e;
+  };
+  if ((e = cudaStreamCreateWithFlags(&hp.s_in, cudaStreamNonBlocking)) != cudaSuccess) return fail();
+  if ((e = cudaStreamCreateWithFlags(&hp.s_comp, cudaStreamNonBlocking)) != cudaSuccess) return fail();
+  if ((e = cudaStreamCreateWithFlags(&hp.s_out, cudaStreamNonBlocking)) != cudaSuccess) return fail();
   for (auto &x : hp.ev)
-    if ((e = cudaEventCreateWithFlags(&x, cudaEventDisableTiming)) != cudaSuccess) return e;
-  if ((e = cudaEventCreateWithFlags(&hp.entry, cudaEventDisableTiming)) != cudaSuccess) return e;
-  if ((e = cudaEventCreateWithFlags(&hp.done_in, cudaEventDisableTiming)) != cudaSuccess) return e;
-  if ((e = cudaEventCreateWithFlags(&hp.done_out, cudaEventDisableTiming)) != cudaSuccess) return e;
+    if ((e = cudaEventCreateWithFlags(&x, cudaEventDisableTiming)) != cudaSuccess) return fail();
+  if ((e = cudaEventCreateWithFlags(&hp.entry, cudaEventDisableTiming)) != cudaSuccess) return fail();
+  if ((e = cudaEventCreateWithFlags(&hp.done_in, cudaEventDisableTiming)) != cudaSuccess) return fail();
+  if ((e = cudaEventCreateWithFlags(&hp.done_out, cudaEventDisableTiming)) != cudaSuccess) return fail();
   hp.live = true;
   return cudaSuccess;
 }
 
+// Destroys every stream and event of the pipe that exists (a partly
+// initialised pipe included) and resets it.
 void host_pipe_destroy(HostPipe &hp) {
-  if (!hp.live) return;
-  cudaStreamDestroy(hp.s_in);
-  cudaStreamDestroy(hp.s_comp);
-  cudaStreamDestroy(hp.s_out);
-  for (auto &x : hp.ev) cudaEventDestroy(x);
-  cudaEventDestroy(hp.entry);
-  cudaEventDestroy(hp.done_in);
-  cudaEventDestroy(hp.done_out);
+  for (cudaStream_t s : {hp.s_in, hp.s_comp, hp.s_out})
+    if (s) cudaStreamDestroy(s);
+  for (auto &x : hp.ev)
+    if (x) cudaEventDestroy(x);
+  for (cudaEvent_t x : {hp.entry, hp.done_in, hp.done_out})
+    if (x) cudaEventDestroy(x);
   hp = HostPipe{};
 }
 
