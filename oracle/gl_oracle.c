@@ -29,6 +29,12 @@
  * w^j), deliberately a different factorisation from the product kernels, and
  * with an O(n^2) definition-based DFT for tiny sizes so tests can pin the
  * fast path.
+ *
+ * Pinning: against the reference's own CUDA kernels, compiled from its
+ * sources into oracle/_ref (GPU tests, same inputs), and without a GPU
+ * against the SHA-256 digests of those kernels' outputs on 176 seeded cases
+ * (tests/golden/, tests/test_golden.py).  Unpinned: boojum's own root of
+ * unity (above), for which no source or vector exists here.
  */
 #include <pthread.h>
 #include <stdint.h>
