@@ -175,16 +175,38 @@ def barrier(world: int):
         dist.barrier()
 
 
-def make_inputs(seed: int):
-    """128 x 2^22 words uniform in [0, p) generated on the device (seeded)."""
+def uniform_words(count: int, seed: int, device: str = "cuda"):
+    """`count` Goldilocks words uniform in [0, p), generated on the device (seeded), as int64 bit patterns.
+
+    A word is two independent uniform 32-bit halves; the words >= p (high half 2^32 - 1 and low half non-zero,
+    about one in 2^32) are drawn again until none is left, so every value in [0, p) is equally likely."""
     import torch
 
-    n = 1 << LOG_N
-    g = torch.Generator(device="cuda").manual_seed(seed)
-    x = torch.randint(-(2**63), 2**63 - 1, (COLS * n,), device="cuda", dtype=torch.int64, generator=g)
-    # words >= p as unsigned are the signed range [-(2^32 - 1), -1]: fold them into [0, p)
-    x = torch.where((x < 0) & (x >= -(2**32 - 1)), x + (2**32 - 1), x)
-    return x
+    g = torch.Generator(device=device).manual_seed(seed)
+
+    def draw(k):
+        hi = torch.randint(0, 2**32, (k,), device=device, dtype=torch.int64, generator=g)
+        lo = torch.randint(0, 2**32, (k,), device=device, dtype=torch.int64, generator=g)
+        return hi, lo
+
+    out = torch.empty(count, device=device, dtype=torch.int64)
+    chunk = 1 << 26
+    for c0 in range(0, count, chunk):
+        k = min(chunk, count - c0)
+        hi, lo = draw(k)
+        bad = ((hi == 2**32 - 1) & (lo != 0)).nonzero().flatten()
+        while bad.numel():
+            h2, l2 = draw(bad.numel())
+            hi[bad], lo[bad] = h2, l2
+            bad = bad[(h2 == 2**32 - 1) & (l2 != 0)]
+        # the high half as a signed 32-bit value keeps the product inside int64
+        out[c0:c0 + k] = torch.where(hi >= 2**31, hi - 2**32, hi) * 2**32 + lo
+    return out
+
+
+def make_inputs(seed: int):
+    """128 x 2^22 words uniform in [0, p) generated on the device (seeded)."""
+    return uniform_words(COLS << LOG_N, seed)
 
 
 def time_steps(fn, steps: int, warmup: int, world: int, stream):
@@ -206,6 +228,88 @@ def time_steps(fn, steps: int, warmup: int, world: int, stream):
     total = evs[0].elapsed_time(evs[-1])
     barrier(world)
     return barrier_max(total, world), per
+
+
+def plan_windows(log_n: int, log_blowup: int):
+    """Window bits of the pass plan the fused LDE uses (top window first), from the loaded plan table; None
+    when the table has no entry (the library's built-in plan)."""
+    import bc_ntt
+
+    for line in bc_ntt.plan_table_export().splitlines():
+        f = line.split()
+        if len(f) >= 3 and int(f[0]) == log_n and int(f[1]) == log_blowup:
+            return [int(f[3 + 2 * i]) for i in range(int(f[2]))]
+    return None
+
+
+def lde_kernel_butterflies(windows, log_n: int, cols: int, log_blowup: int):
+    """Radix-2 butterflies of each kernel of the fused LDE, in launch order: the inverse passes below the top
+    window (bottom-up), the top-window kernel (inverse stages once, forward stages for every coset), the forward
+    passes below it (every coset)."""
+    half, B = (1 << log_n) // 2 * cols, 1 << log_blowup
+    below = windows[1:]
+    return ([k * half for k in reversed(below)] + [windows[0] * (1 + B) * half] + [k * B * half for k in below])
+
+
+def butterfly_peak(target_ms: float = 40.0, reps: int = 3):
+    """Butterflies per second of the transform kernels' round arithmetic alone, from registers, in every resident
+    thread slot (bc_butterfly_peak): the 32-bit integer issue roofline.  Best of `reps` launches of about
+    `target_ms` each, CUDA events on the current stream.  Returns (G butterflies/s, launch ms)."""
+    import ctypes
+
+    import torch
+
+    import bc_ntt
+
+    L = bc_ntt.lib()
+    words = ctypes.c_size_t(0)
+    assert L.bc_butterfly_peak_words(ctypes.byref(words)) == 0
+    out = torch.empty(words.value, dtype=torch.int64, device="cuda")
+    stream = torch.cuda.current_stream()
+    bfly = ctypes.c_uint64(0)
+
+    def launch(iters):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        rc = L.bc_butterfly_peak(out.data_ptr(), words.value, iters, stream.cuda_stream, ctypes.byref(bfly))
+        assert rc == 0, rc
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b)
+
+    iters = 64
+    ms = launch(iters)
+    iters = max(1, int(iters * target_ms / max(ms, 1e-3)))
+    best = None
+    for _ in range(reps):
+        ms = launch(iters)
+        rate = bfly.value / (ms / 1e3) / 1e9
+        best = (rate, ms) if best is None or rate > best[0] else best
+    del out
+    return best
+
+
+def lde_matches_fused(ev, out, log_n: int, cols: int, log_blowup: int, chunk_words: int = 1 << 28) -> bool:
+    """True when `out`, the dense coset-major LDE of `ev` (device tensors), equals bc_lde_fused's result bit for
+    bit.  The reference result is computed again column chunk by column chunk into a scratch buffer of at most
+    `chunk_words` words, so any job size is checked in bounded memory."""
+    import torch
+
+    import bc_ntt
+
+    L = bc_ntt.lib()
+    n, B = 1 << log_n, 1 << log_blowup
+    chunk = max(1, min(cols, chunk_words // (B * n)))
+    tmp = torch.empty(B * chunk * n, dtype=torch.int64, device="cuda")
+    s = torch.cuda.current_stream().cuda_stream
+    view = out.view(B, cols, n)
+    for c0 in range(0, cols, chunk):
+        k = min(chunk, cols - c0)
+        rc = L.bc_lde_fused(ev.data_ptr() + 8 * c0 * n, tmp.data_ptr(), log_n, k, n, n, k * n, log_blowup, s)
+        assert rc == 0, rc
+        if not torch.equal(view[:, c0:c0 + k], tmp[:B * k * n].view(B, k, n)):
+            return False
+    return True
 
 
 def pct(xs, q):
@@ -254,8 +358,7 @@ def run_small_ntt_section(call, reps: int = 200, log_n: int = 16, cols: int = 16
 
     n = 1 << log_n
     stream = torch.cuda.current_stream()
-    g = torch.Generator(device="cuda").manual_seed(16)
-    x = torch.randint(0, 2**62, (cols * n,), dtype=torch.int64, device="cuda", generator=g)
+    x = uniform_words(cols * n, 16)
     y = torch.empty_like(x)
     for _ in range(20):
         call(x.data_ptr(), y.data_ptr(), log_n, cols, stream.cuda_stream)
@@ -382,22 +485,40 @@ def run_ours(args, rank, world):
                + [(f"lde forward pass {i} (n2b, all cosets)", 2 * B * col_bytes) for i in range(npass - 1)])
     roofline = None
     traffic, alu_pct, fma_pct = measured_traffic(LOG_N, LOG_BLOWUP, COLS)
+    peak_bfly, peak_ms = butterfly_peak()
+    windows = plan_windows(LOG_N, LOG_BLOWUP)
+    kbfly = lde_kernel_butterflies(windows, LOG_N, COLS, LOG_BLOWUP) if windows else None
     if kern_ms and len(kern_ms) == len(kernels):
         dom = max(range(len(kern_ms)), key=lambda i: kern_ms[i])
         name, byts = kernels[dom]
         achieved = byts / (kern_ms[dom] / 1e3) / 1e9
         top = "lde_top_kernel" in name
-        roofline = {"bound": "hbm", "kernel": name, "achieved": round(achieved, 1), "peak": peak,
+        # The HBM roofline of the kernel's algorithmic bytes (achieved / peak / frac) is reported as the contract
+        # asks, but it does not bound these kernels: (1 + B) (n / 2) log n butterflies of 64-bit modular arithmetic
+        # on 32-bit integer pipes do.  `limiter` is that roofline: butterflies per second of the kernel against
+        # the same round arithmetic run from registers (bc_butterfly_peak, measured in this run).
+        roofline = {"bound": "int32 issue", "kernel": name, "achieved": round(achieved, 1), "peak": peak,
                     "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+                    "hbm_frac_note": "achieved/peak/frac: HBM roofline of the algorithmic bytes; see limiter",
                     "spec_frac": round(achieved / SPEC_HBM_GBS, 4),
                     "traffic": traffic if top else None,
                     "traffic_unit": "bytes per launch (ncu dram read+write, scaled from the profiled case)",
                     "kernel_ms": [round(v, 3) for v in kern_ms],
                     "step_algorithmic_frac": round(8 * n * COLS * (1 + B) / (ms_per_step / 1e3) / 1e9 / peak, 4)}
-        if top and alu_pct is not None:
-            # what bounds the kernel instead of HBM: 32-bit integer issue (ncu capture of the same kernel)
-            roofline["limiter"] = {"kind": "int32 issue", "alu_pipe_pct": alu_pct, "fma_pipe_pct": fma_pct,
-                                   "source": "ncu --set full, profiles/lde_kernels_ncu_full_8cols_logn22_blowup2.md"}
+        if kbfly and len(kbfly) == len(kern_ms):
+            rates = [b / (t / 1e3) / 1e9 for b, t in zip(kbfly, kern_ms)]
+            step_rate = sum(kbfly) / (ms_per_step / 1e3) / 1e9
+            roofline["limiter"] = {
+                "bound": "int32 issue", "unit": "G butterflies/s", "kernel": name,
+                "achieved": round(rates[dom], 1), "peak": round(peak_bfly, 1),
+                "frac": round(rates[dom] / peak_bfly, 4),
+                "per_kernel_achieved": [round(r, 1) for r in rates],
+                "step_achieved": round(step_rate, 1), "step_frac": round(step_rate / peak_bfly, 4),
+                "butterflies_per_step": sum(kbfly), "plan_windows": windows,
+                "peak_source": f"bc_butterfly_peak: the kernels' radix-16 round arithmetic from registers, every "
+                               f"resident thread slot, best of 3 launches of {peak_ms:.1f} ms, this run",
+                "alu_pipe_pct": alu_pct, "fma_pipe_pct": fma_pct,
+                "pipe_source": "ncu of the top-window kernel, profiles/lde_kernels_ncu_full_8cols_logn22_blowup2.md"}
 
     # end to end through the C ABI with host buffers: bc_lde_host takes pinned host input and writes pinned
     # host output every step, overlapping chunked copy-in / transform / copy-out on three streams
@@ -470,9 +591,7 @@ def _uneven_tensors(specs):
 
     tens = []
     for sp in specs:
-        g = torch.Generator(device="cuda").manual_seed(sp.seed)
-        ev = torch.randint(-(2**63), 2**63 - 1, (sp.in_words,), device="cuda", dtype=torch.int64, generator=g)
-        ev = torch.where((ev < 0) & (ev >= -(2**32 - 1)), ev + (2**32 - 1), ev)  # uniform in [0, p)
+        ev = uniform_words(sp.in_words, sp.seed)
         tens.append((ev, torch.empty(sp.out_words, dtype=torch.int64, device="cuda"), sp.log_n, sp.cols,
                      sp.log_blowup))
     return tens
@@ -504,21 +623,38 @@ def run_batch_section(reps: int = 3):
     out_elems = sum(sp.out_words for sp in specs)
     t_batch = timed(plan.run)
     status = plan.status()
+    # every output of every job, bit for bit against the same job alone through bc_lde_fused
+    exact_persistent = sum(lde_matches_fused(*t) for t in tens)
     # hybrid: jobs whose kernels span >= 4 waves of CTAs run as their own kernels in the same graph
     hybrid = bc_ntt.LdeBatch(tens, standalone_min_ctas=4 * 2 * torch.cuda.get_device_properties(0).multi_processor_count)
+    for t in tens:
+        t[1].zero_()
     t_hybrid = timed(hybrid.run)
     status |= hybrid.status()
     hybrid.close()
-    batch_out = [t[1].clone() for t in tens[:8]]
+    exact_hybrid = sum(lde_matches_fused(*t) for t in tens)
     t_fused = timed(lambda: [bc_ntt.lde(*t, fused=True) for t in tens])
-    exact = all(torch.equal(a, t[1]) for a, t in zip(batch_out, tens[:8]))
     t_plain = timed(lambda: [bc_ntt.lde(*t, fused=False) for t in tens])
     info = plan.info()
     plan.close()
-    del tens, batch_out
+    # the jobs the reference's kernels can run (log_n + log2 B <= 24): the same paths, for the reference arm's
+    # per-job composition on the same subset
+    sub = [t for t, sp in zip(tens, specs) if reference_can_run(sp)]
+    sub_plan = bc_ntt.LdeBatch(sub)
+    t_sub_batch = timed(sub_plan.run)
+    status |= sub_plan.status()
+    sub_plan.close()
+    t_sub_fused = timed(lambda: [bc_ntt.lde(*t, fused=True) for t in sub])
+    t_sub_plain = timed(lambda: [bc_ntt.lde(*t, fused=False) for t in sub])
+    sub_elems = sum(sp.out_words for sp in specs if reference_can_run(sp))
+    del sub
+    del tens
     torch.cuda.empty_cache()
     mel = lambda ms: round(out_elems / (ms / 1e3) / 1e6, 1)  # noqa: E731
     return {"workload": "96 jobs, log_n U{12..22}, cols log-U[1,256], blowup U{2,4,8}, seed 42",
+            "bit_exact_all_96": exact_persistent == len(specs) and exact_hybrid == len(specs),
+            "jobs_exact": {"persistent": exact_persistent, "hybrid": exact_hybrid, "of": len(specs),
+                           "against": "each job alone through bc_lde_fused, every output word"},
             "total_out_gelem": round(out_elems / 1e9, 2),
             "persistent_one_launch": {"ms": round(t_batch, 2), "value": mel(t_batch), "status": status,
                                       "records": info["records"], "items": info["items"], "grid": info["grid"]},
@@ -527,8 +663,58 @@ def run_batch_section(reps: int = 3):
             "per_job_fused": {"ms": round(t_fused, 2), "value": mel(t_fused)},
             "per_job_plain": {"ms": round(t_plain, 2), "value": mel(t_plain)},
             "persistent_vs_plain": round(t_plain / t_batch, 3), "hybrid_vs_plain": round(t_plain / t_hybrid, 3),
-            "fused_vs_plain": round(t_plain / t_fused, 3),
-            "bit_exact_persistent_vs_per_job": bool(exact), "unit": "Melem/s"}
+            "fused_vs_plain": round(t_plain / t_fused, 3), "unit": "Melem/s",
+            "reference_subset": {"jobs": sum(reference_can_run(sp) for sp in specs), "rule": "log_n + log2 B <= 24",
+                                 "out_gelem": round(sub_elems / 1e9, 3),
+                                 "persistent_ms": round(t_sub_batch, 2), "per_job_fused_ms": round(t_sub_fused, 2),
+                                 "per_job_plain_ms": round(t_sub_plain, 2),
+                                 "note": "the reference arm times its own per-job composition on these jobs"}}
+
+
+def reference_can_run(spec) -> bool:
+    """The reference's kernels cover transforms with log_n + log_extension_degree <= 24 (src/context.rs:12)."""
+    return spec.log_n + spec.log_blowup <= 24
+
+
+def run_reference_batch_section(ref, reps: int = 3):
+    """The 96-job uneven workload as the reference's callers run it, one job at a time: per job one inverse
+    batch_ntt, then one forward batch_ntt per coset (src/ntt.rs:179-290; log_n < 16 goes through its per-stage
+    launches), on the jobs its kernels cover (log_n + log2 B <= 24)."""
+    import torch
+
+    import workloads
+
+    specs = [sp for sp in workloads.uneven_batch(n_jobs=96, seed=42) if reference_can_run(sp)]
+    tens = _uneven_tensors(specs)
+    stream = torch.cuda.current_stream()
+    s = stream.cuda_stream
+
+    def job(ev, out, log_n, cols, log_b):
+        n, B = 1 << log_n, 1 << log_b
+        coef = out.data_ptr() + 8 * (B - 1) * cols * n
+        ref.batch_ntt(ev.data_ptr(), coef, log_n, cols, n, n, True, True, 0, 0, s)
+        for k in range(B):
+            ref.batch_ntt(coef, out.data_ptr() + 8 * k * cols * n, log_n, cols, n, n, False, False, log_b, k, s)
+
+    def all_jobs():
+        for t in tens:
+            job(*t)
+
+    all_jobs()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(reps):
+        all_jobs()
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / reps
+    out_elems = sum(sp.out_words for sp in specs)
+    del tens
+    torch.cuda.empty_cache()
+    return {"workload": "the 96-job uneven batch (seed 42), jobs with log_n + log2 B <= 24", "jobs": len(specs),
+            "out_gelem": round(out_elems / 1e9, 3), "per_job_reference_ms": round(ms, 2),
+            "value": round(out_elems / (ms / 1e3) / 1e6, 1), "unit": "Melem/s"}
 
 
 def run_small_batch_section(reps: int = 5):
@@ -581,9 +767,7 @@ def run_large_section(reps: int = 5):
 
     log_n, cols, log_b = 23, 64, 2
     n, B = 1 << log_n, 1 << log_b
-    g = torch.Generator(device="cuda").manual_seed(77)
-    x = torch.randint(-(2**63), 2**63 - 1, (cols * n,), device="cuda", dtype=torch.int64, generator=g)
-    x = torch.where((x < 0) & (x >= -(2**32 - 1)), x + (2**32 - 1), x)
+    x = uniform_words(cols * n, 77)
     out = torch.empty(B * cols * n, dtype=torch.int64, device="cuda")
     stream = torch.cuda.current_stream()
 
@@ -725,11 +909,15 @@ def ops_reference(ref):
     }
 
 
-def run_serve_section(n_requests: int = 48, rate: float = 20.0, budget_gib: int = 40, slots: int = 4):
+def run_serve_section(n_requests: int = 24, rates=(10.0, 20.0), budget_gib: int = 40, slots: int = 4):
     """Poisson LDE requests through the continuous-batching server vs the same requests served one at a time.
 
-    latency: requests arrive at `rate`/s; p50/p99 of completion - arrival, beside the FCFS one-at-a-time
-             plain path fed the same arrivals (its queueing computed from measured per-request service times).
+    Every request has its own pinned host input and output region (carved from two pinned pools), and after every
+    server run each request's output is checked, bit for bit, against the same request computed alone on the
+    device through bc_lde_fused.
+    latency: requests arrive at each rate in `rates` (the seeded Poisson arrivals scaled to that rate); p50/p99 of
+             completion - arrival, beside the FCFS one-at-a-time plain path fed the same arrivals (its queueing
+             computed from measured per-request service times).
     capacity: all requests queued at once; output Melem/s of the server vs the one-at-a-time plain path.
     """
     import torch
@@ -737,68 +925,104 @@ def run_serve_section(n_requests: int = 48, rate: float = 20.0, budget_gib: int 
     import bc_ntt
     import workloads
 
-    reqs = workloads.serving_stream(n_requests=n_requests, rate_per_s=rate, seed=7)
-    max_in = max(r.in_words for r in reqs)
-    max_out = max(r.out_words for r in reqs)
-    out_elems = sum(r.out_words for r in reqs)
-    # host pools reused by every request (timing; per-request exactness is covered by tests/test_server_gpu.py)
-    hin = torch.randint(0, 2**62, (max_in,), dtype=torch.int64).pin_memory()
-    hout = torch.empty(max_out, dtype=torch.int64).pin_memory()
+    reqs = workloads.serving_stream(n_requests=n_requests, rate_per_s=rates[0], seed=7)
+    in_off, out_off, a, b = [], [], 0, 0
+    for r in reqs:
+        in_off.append(a)
+        out_off.append(b)
+        a += r.in_words
+        b += r.out_words
+    out_elems = b
+    t_pin = time.perf_counter()
+    hin = torch.empty(a, dtype=torch.int64, pin_memory=True)
+    hout = torch.empty(b, dtype=torch.int64, pin_memory=True)
+    pin_s = time.perf_counter() - t_pin
+    # inputs uniform in [0, p) (each request its own seed); the expected outputs stay on the device
+    expected = []
+    for r, o in zip(reqs, in_off):
+        ev = uniform_words(r.in_words, r.seed)
+        hin[o:o + r.in_words].copy_(ev)
+        exp = torch.empty(r.out_words, dtype=torch.int64, device="cuda")
+        bc_ntt.lde(ev, exp, r.log_n, r.cols, r.log_blowup, fused=True)
+        expected.append(exp)
+        del ev
+    torch.cuda.synchronize()
+
+    def exact_requests() -> int:
+        """Requests whose host output region equals their expected output, word for word."""
+        good = 0
+        for r, o, exp in zip(reqs, out_off, expected):
+            good += int(torch.equal(hout[o:o + r.out_words].to("cuda", non_blocking=True), exp))
+        return good
 
     # one at a time through the plain path: copy in, bc_lde_plain, copy out; service time of each request
+    max_in = max(r.in_words for r in reqs)
+    max_out = max(r.out_words for r in reqs)
     dev_in = torch.empty(max_in, dtype=torch.int64, device="cuda")
     dev_out = torch.empty(max_out, dtype=torch.int64, device="cuda")
     stream = torch.cuda.current_stream()
     evs = [torch.cuda.Event(enable_timing=True) for _ in range(len(reqs) + 1)]
+    hout.zero_()
     torch.cuda.synchronize()
     evs[0].record(stream)
     for i, r in enumerate(reqs):
-        dev_in[:r.in_words].copy_(hin[:r.in_words], non_blocking=True)
+        dev_in[:r.in_words].copy_(hin[in_off[i]:in_off[i] + r.in_words], non_blocking=True)
         bc_ntt.lde(dev_in, dev_out, r.log_n, r.cols, r.log_blowup, fused=False)
-        hout[:r.out_words].copy_(dev_out[:r.out_words], non_blocking=True)
+        hout[out_off[i]:out_off[i] + r.out_words].copy_(dev_out[:r.out_words], non_blocking=True)
         evs[i + 1].record(stream)
     torch.cuda.synchronize()
     service = [evs[i].elapsed_time(evs[i + 1]) for i in range(len(reqs))]
     serial_s = sum(service) / 1e3
+    exact = {"serial_plain": exact_requests()}
     del dev_in, dev_out
     torch.cuda.empty_cache()
-    # FCFS single-server latencies of the plain path under the same arrivals
-    t_free, lat_serial = 0.0, []
-    for r, sv in zip(reqs, service):
-        start = max(r.arrival_s * 1e3, t_free)
-        t_free = start + sv
-        lat_serial.append(t_free - r.arrival_s * 1e3)
 
     def serve(arrivals):
+        hout.zero_()
         srv = bc_ntt.LdeServer(memory_budget_bytes=budget_gib << 30, slots=slots)
         t0 = time.perf_counter()
         ids = []
-        for r, at in zip(reqs, arrivals):
+        for i, (r, at) in enumerate(zip(reqs, arrivals)):
             d = t0 + at - time.perf_counter()
             if d > 0:
                 time.sleep(d)
-            ids.append(srv.submit(hin, hout, r.log_n, r.cols, r.log_blowup))
+            ids.append(srv.submit(hin[in_off[i]:in_off[i] + r.in_words], hout[out_off[i]:out_off[i] + r.out_words],
+                                  r.log_n, r.cols, r.log_blowup))
         for i in ids:
             srv.wait(i, timeout_ms=600000)
         st = srv.stats()
         srv.close()
         return st
 
-    st_lat = serve([r.arrival_s for r in reqs])
-    st_cap = serve([0.0] * len(reqs))
-    del hin, hout
-    return {"workload": f"{n_requests} requests, log_n U{{14..22}}, cols log-U[8,512], blowup U{{2,4}}, seed 7, "
-                        f"pinned host buffers, {budget_gib} GiB budget, {slots} slots",
-            "unit": "Melem/s",
-            "latency": {"rate_per_s": rate, "p50_ms": round(st_lat["p50_ms"], 2), "p99_ms": round(st_lat["p99_ms"], 2),
-                        "max_ms": round(st_lat["max_ms"], 2),
+    latency = []
+    for rate in rates:
+        arrivals = [r.arrival_s * rates[0] / rate for r in reqs]
+        st = serve(arrivals)
+        exact[f"rate_{rate:g}"] = exact_requests()
+        # FCFS single-server latencies of the plain path under the same arrivals
+        t_free, lat_serial = 0.0, []
+        for at, sv in zip(arrivals, service):
+            start = max(at * 1e3, t_free)
+            t_free = start + sv
+            lat_serial.append(t_free - at * 1e3)
+        latency.append({"rate_per_s": rate, "p50_ms": round(st["p50_ms"], 2), "p99_ms": round(st["p99_ms"], 2),
+                        "max_ms": round(st["max_ms"], 2), "completed": int(st["completed"]),
                         "serial_plain_same_arrivals_p50_ms": round(pct(lat_serial, 50), 2),
-                        "serial_plain_same_arrivals_p99_ms": round(pct(lat_serial, 99), 2)},
+                        "serial_plain_same_arrivals_p99_ms": round(pct(lat_serial, 99), 2)})
+    st_cap = serve([0.0] * len(reqs))
+    exact["capacity"] = exact_requests()
+    del hin, hout, expected
+    torch.cuda.empty_cache()
+    return {"workload": f"{n_requests} requests, log_n U{{14..22}}, cols log-U[8,512], blowup U{{2,4}}, seed 7, "
+                        f"per-request pinned host buffers, {budget_gib} GiB budget, {slots} slots",
+            "unit": "Melem/s", "total_out_gelem": round(out_elems / 1e9, 3), "pin_s": round(pin_s, 2),
+            "bit_exact": all(v == len(reqs) for v in exact.values()),
+            "requests_exact": dict(exact, of=len(reqs), against="each request alone through bc_lde_fused"),
+            "latency": latency,
             "capacity": {"server_value": round(st_cap["out_melem_per_s"], 1),
                          "serial_plain_value": round(out_elems / serial_s / 1e6, 1),
                          "speedup": round(st_cap["out_melem_per_s"] / (out_elems / serial_s / 1e6), 3),
-                         "server_span_s": round(st_cap["span_s"], 3), "serial_plain_s": round(serial_s, 3)},
-            "completed": int(st_lat["completed"] + st_cap["completed"])}
+                         "server_span_s": round(st_cap["span_s"], 3), "serial_plain_s": round(serial_s, 3)}}
 
 
 def run_reference(args, rank, world):
@@ -866,6 +1090,8 @@ def run_reference(args, rank, world):
     }
     if small is not None:
         line["small_ntt"] = small
+    if world == 1 and not args.no_batch:
+        line["batch_per_job_reference"] = run_reference_batch_section(ref)
     if ops is not None:
         line["ops"] = ops
     return line

@@ -63,7 +63,10 @@ SIGNATURES = {
     "bc_lde_batch_plan_create_ex": [_vp, _u32, _u32, _vp],
     "bc_lde_batch_run": [_vp, _vp],
     "bc_lde_batch_status": [_vp, _vp, _vp],
+    "bc_lde_batch_plan_set_wait_limit": [_vp, _u64],
     "bc_lde_batch_plan_info": [_vp, _vp, _vp, _vp],
+    "bc_butterfly_peak_words": [_vp],
+    "bc_butterfly_peak": [_vp, _sz, _u32, _vp, _vp],
     "bc_lde_batch_plan_destroy": [_vp],
     "bc_lde_batch_noalloc": [_vp, _u32, _vp, _vp],
     "bc_lde_server_create": [_vp, _vp],
@@ -250,6 +253,10 @@ class LdeBatch:
         st = ctypes.c_uint32(0)
         _check(lib().bc_lde_batch_status(self.handle, _stream(stream), ctypes.byref(st)), "bc_lde_batch_status")
         return st.value
+
+    def set_wait_limit(self, cycles: int):
+        """SM clock cycles one dependency wait of the persistent kernel may take (0: the default, about 4 s)."""
+        _check(lib().bc_lde_batch_plan_set_wait_limit(self.handle, cycles), "bc_lde_batch_plan_set_wait_limit")
 
     def info(self):
         r, i, g = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()

@@ -23,6 +23,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cstdint>
 #include <cstring>
 #include <mutex>
@@ -107,12 +108,14 @@ __device__ __forceinline__ uint32_t ld_acquire(const uint32_t *p) {
 }
 
 // status bit 0: a dependency wait expired (the batch's results are invalid).
+// wait_limit: SM clock cycles one dependency wait may take (read once per CTA).
 __global__ void __launch_bounds__(BATCH_THREADS, 2)
     lde_batch_kernel(const BatchRecord *__restrict__ recs, const uint64_t *__restrict__ items, uint32_t n_items,
-                     uint32_t *done, uint32_t *next, uint32_t *status, long long timeout_cycles) {
+                     uint32_t *done, uint32_t *next, uint32_t *status, const long long *wait_limit) {
   extern __shared__ uint64_t smem[];
   __shared__ uint32_t s_idx, s_ok;
   __shared__ BatchRecord s_rec; // the item's kernel parameters, read by the body from shared memory
+  const long long timeout_cycles = threadIdx.x == 0 ? *wait_limit : 0;
   for (;;) {
     if (threadIdx.x == 0) s_idx = atomicAdd(next, 1u);
     __syncthreads();
@@ -159,11 +162,25 @@ struct bc_lde_batch_plan {
   uint32_t n_records = 0, n_items = 0, grid = 0;
   BatchRecord *d_records = nullptr;
   uint64_t *d_items = nullptr;
-  uint32_t *d_counters = nullptr; // done[n_records], next, status
+  uint32_t *d_counters = nullptr; // done[n_records], next, status, then the 64-bit wait limit (8-byte aligned)
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   long long timeout_cycles = 0;
 };
+
+namespace {
+// Words of a counters block for n_records records: done[], next, status, padding to 8 bytes, the wait limit.
+uint32_t counter_words(uint32_t n_records) { return ((n_records + 2 + 1) & ~1u) + 2; }
+long long *wait_limit_slot(uint32_t *counters, uint32_t n_records) {
+  return reinterpret_cast<long long *>(counters + counter_words(n_records) - 2);
+}
+// About 4 s of SM clock per dependency wait.
+long long default_wait_limit(int device) {
+  int clock_khz = 0;
+  cudaDeviceGetAttribute(&clock_khz, cudaDevAttrClockRate, device);
+  return (long long)std::max(clock_khz, 1000000) * 1000ll * 4;
+}
+} // namespace
 
 namespace {
 
@@ -181,13 +198,24 @@ cudaError_t free_plan(bc_lde_batch_plan *p) {
 
 uint64_t job_work(const bc_lde_job &j) { return ((uint64_t)j.num_cols << j.log_n) << j.log_blowup; }
 
+size_t round256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// Device bytes of a schedule laid out as counters (done[n_records], next,
+// status) | records | items, each part 256-byte aligned.
+size_t schedule_bytes(size_t n_records, size_t n_items) {
+  return round256((((n_records + 3) & ~(size_t)1) + 2) * sizeof(uint32_t)) +
+         round256(n_records * sizeof(BatchRecord)) + n_items * sizeof(uint64_t);
+}
+
 // Records and items of a batch, in dependency order (host side).
 // standalone_min_ctas > 0: a job whose every kernel, launched on its own, has
 // at least that many CTAs goes to `standalone` (its fused-LDE steps in order)
 // instead of the persistent kernel's schedule.
+// max_bytes > 0: a schedule needing more device bytes (schedule_bytes) returns
+// cudaErrorInvalidValue before any record or item is built.
 cudaError_t schedule(const bc_lde_job *jobs, uint32_t n_jobs, std::vector<BatchRecord> &recs,
                      std::vector<uint64_t> &items, uint32_t standalone_min_ctas = 0,
-                     std::vector<LdeStep> *standalone = nullptr) {
+                     std::vector<LdeStep> *standalone = nullptr, size_t max_bytes = 0) {
   std::vector<std::vector<LdeStep>> steps(n_jobs);
   size_t max_depth = 0;
   for (uint32_t j = 0; j < n_jobs; j++) {
@@ -222,6 +250,16 @@ cudaError_t schedule(const bc_lde_job *jobs, uint32_t n_jobs, std::vector<BatchR
     if (!build(tuned_plan(jb.log_n, jb.log_blowup)) && !build(default_plan(jb.log_n)))
       return cudaErrorInvalidConfiguration;
     max_depth = std::max(max_depth, steps[j].size());
+  }
+  if (max_bytes) {
+    uint64_t n_recs = 0, n_items = 0;
+    for (uint32_t j = 0; j < n_jobs; j++)
+      for (const LdeStep &st : steps[j]) {
+        n_recs++;
+        n_items += (uint64_t)st.grid.x * st.grid.y;
+      }
+    if (n_items > max_bytes / sizeof(uint64_t) || schedule_bytes(n_recs, n_items) > max_bytes)
+      return cudaErrorInvalidValue;
   }
   // big jobs first within every depth
   std::vector<uint32_t> order(n_jobs);
@@ -273,9 +311,7 @@ extern "C" cudaError_t bc_lde_batch_plan_create_ex(const bc_lde_job *jobs, uint3
   p->device = current_device();
   p->n_records = (uint32_t)recs.size();
   p->n_items = (uint32_t)items.size();
-  int dev_clock_khz = 0;
-  cudaDeviceGetAttribute(&dev_clock_khz, cudaDevAttrClockRate, p->device);
-  p->timeout_cycles = (long long)std::max(dev_clock_khz, 1000000) * 1000ll * 4; // ~4 s of SM clock per wait
+  p->timeout_cycles = default_wait_limit(p->device);
 #define CK(x)                                                                                                          \
   if ((e = (x)) != cudaSuccess) {                                                                                      \
     free_plan(p);                                                                                                      \
@@ -295,8 +331,10 @@ extern "C" cudaError_t bc_lde_batch_plan_create_ex(const bc_lde_job *jobs, uint3
     CK(cudaMalloc(&p->d_items, items.size() * sizeof(uint64_t)));
     CK(cudaMemcpy(p->d_items, items.data(), items.size() * sizeof(uint64_t), cudaMemcpyHostToDevice));
   }
-  CK(cudaMalloc(&p->d_counters, (p->n_records + 2) * sizeof(uint32_t)));
+  CK(cudaMalloc(&p->d_counters, counter_words(p->n_records) * sizeof(uint32_t)));
   CK(cudaMemset(p->d_counters, 0, (p->n_records + 2) * sizeof(uint32_t)));
+  CK(cudaMemcpy(wait_limit_slot(p->d_counters, p->n_records), &p->timeout_cycles, sizeof(long long),
+                cudaMemcpyHostToDevice));
   // capture: reset the counters, run the persistent kernel; the standalone jobs'
   // kernels run on a forked branch of the same graph, concurrently with it
   cudaStream_t cs, cs2;
@@ -317,7 +355,7 @@ extern "C" cudaError_t bc_lde_batch_plan_create_ex(const bc_lde_job *jobs, uint3
     if (ec == cudaSuccess && p->n_items) {
       lde_batch_kernel<<<p->grid, BATCH_THREADS, BATCH_SMEM_BYTES, cs>>>(
           p->d_records, p->d_items, p->n_items, p->d_counters, p->d_counters + p->n_records,
-          p->d_counters + p->n_records + 1, p->timeout_cycles);
+          p->d_counters + p->n_records + 1, wait_limit_slot(p->d_counters, p->n_records));
       ec = cudaGetLastError();
     }
     if (ec == cudaSuccess && !standalone.empty()) ec = cudaStreamWaitEvent(cs, join, 0);
@@ -354,6 +392,17 @@ extern "C" cudaError_t bc_lde_batch_status(bc_lde_batch_plan *plan, cudaStream_t
                                   cudaMemcpyDeviceToHost, stream);
   if (e != cudaSuccess) return e;
   return cudaStreamSynchronize(stream);
+}
+
+extern "C" cudaError_t bc_lde_batch_plan_set_wait_limit(bc_lde_batch_plan *plan, uint64_t cycles) {
+  if (!plan || cycles > (uint64_t)LLONG_MAX) return cudaErrorInvalidValue;
+  if (current_device() != plan->device) return cudaErrorInvalidDevice;
+  const long long v = cycles ? (long long)cycles : default_wait_limit(plan->device);
+  // runs already enqueued (on any stream) finish with the old limit; later ones read the new one
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaMemcpy(wait_limit_slot(plan->d_counters, plan->n_records), &v, sizeof(v), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) plan->timeout_cycles = v;
+  return e;
 }
 
 extern "C" cudaError_t bc_lde_batch_plan_info(const bc_lde_batch_plan *plan, uint32_t *n_records, uint32_t *n_items,
@@ -411,30 +460,34 @@ cudaError_t noalloc_setup(int dev, void **base, int *grid) {
   *grid = g_noalloc_grid[dev];
   return cudaSuccess;
 }
-
-size_t round256(size_t x) { return (x + 255) & ~(size_t)255; }
 } // namespace
 } // namespace bc
 
 extern "C" cudaError_t bc_lde_batch_noalloc(const bc_lde_job *jobs, uint32_t n_jobs, cudaStream_t stream,
                                             uint32_t *status) {
   if (n_jobs && !jobs) return cudaErrorInvalidValue;
+  // The schedule is copied from host vectors that this call frees on return,
+  // and `status` synchronises the stream: neither can be recorded into a graph.
+  cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+  cudaError_t e = cudaStreamIsCapturing(stream, &capture);
+  if (e != cudaSuccess) return e;
+  if (capture != cudaStreamCaptureStatusNone) return cudaErrorStreamCaptureUnsupported;
   if (!device_tables()) return cudaErrorInitializationError;
   const int dev = current_device();
   if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return cudaErrorInvalidDevice;
   void *base = nullptr;
   int grid = 0;
-  cudaError_t e = noalloc_setup(dev, &base, &grid);
+  e = noalloc_setup(dev, &base, &grid);
   if (e != cudaSuccess) return e;
   std::vector<BatchRecord> recs;
   std::vector<uint64_t> items;
-  e = schedule(jobs, n_jobs, recs, items);
+  e = schedule(jobs, n_jobs, recs, items, 0, nullptr, NOALLOC_SCRATCH_BYTES);
   if (e != cudaSuccess) return e;
-  // layout: counters (done[n_records], next, status) | records | items
-  const size_t counters_bytes = round256((recs.size() + 2) * sizeof(uint32_t));
+  // layout: counters (done[n_records], next, status, wait limit) | records | items
+  const size_t counters_bytes = round256(counter_words((uint32_t)recs.size()) * sizeof(uint32_t));
   const size_t recs_bytes = round256(recs.size() * sizeof(BatchRecord));
   const size_t items_bytes = items.size() * sizeof(uint64_t);
-  if (counters_bytes + recs_bytes + items_bytes > NOALLOC_SCRATCH_BYTES) return cudaErrorInvalidValue;
+  if (schedule_bytes(recs.size(), items.size()) > NOALLOC_SCRATCH_BYTES) return cudaErrorInvalidValue;
   unsigned char *b = static_cast<unsigned char *>(base);
   uint32_t *counters = reinterpret_cast<uint32_t *>(b);
   BatchRecord *d_recs = reinterpret_cast<BatchRecord *>(b + counters_bytes);
@@ -448,13 +501,14 @@ extern "C" cudaError_t bc_lde_batch_noalloc(const bc_lde_job *jobs, uint32_t n_j
     if (e != cudaSuccess) return e;
     e = cudaMemcpyAsync(d_items, items.data(), items_bytes, cudaMemcpyHostToDevice, stream);
     if (e != cudaSuccess) return e;
-    int clock_khz = 0;
-    cudaDeviceGetAttribute(&clock_khz, cudaDevAttrClockRate, dev);
-    const long long timeout = (long long)std::max(clock_khz, 1000000) * 1000ll * 4;
     const uint32_t n_rec = (uint32_t)recs.size();
+    const long long limit = default_wait_limit(dev);
+    e = cudaMemcpyAsync(wait_limit_slot(counters, n_rec), &limit, sizeof(limit), cudaMemcpyHostToDevice, stream);
+    if (e != cudaSuccess) return e;
     lde_batch_kernel<<<grid, BATCH_THREADS, BATCH_SMEM_BYTES, stream>>>(d_recs, d_items, (uint32_t)items.size(),
                                                                          counters, counters + n_rec,
-                                                                         counters + n_rec + 1, timeout);
+                                                                         counters + n_rec + 1,
+                                                                         wait_limit_slot(counters, n_rec));
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }

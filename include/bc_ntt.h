@@ -183,6 +183,12 @@ cudaError_t bc_lde_batch_plan_create_ex(const bc_lde_job *jobs, uint32_t n_jobs,
 cudaError_t bc_lde_batch_run(bc_lde_batch_plan *plan, cudaStream_t stream);
 /* Waits for the stream, then returns the status word of the plan's last run. */
 cudaError_t bc_lde_batch_status(bc_lde_batch_plan *plan, cudaStream_t stream, uint32_t *status);
+/* Sets how long one dependency wait of the plan's persistent kernel may take,
+ * in SM clock cycles (0: the default, about 4 s).  A wait that runs out sets
+ * status bit 0, skips its work item and lets the kernel finish, so a stalled
+ * dependency ends as an error status instead of a hung GPU.  Waits for the
+ * device first; later runs use the new limit. */
+cudaError_t bc_lde_batch_plan_set_wait_limit(bc_lde_batch_plan *plan, uint64_t cycles);
 cudaError_t bc_lde_batch_plan_info(const bc_lde_batch_plan *plan, uint32_t *n_records, uint32_t *n_items,
                                    uint32_t *grid);
 cudaError_t bc_lde_batch_plan_destroy(bc_lde_batch_plan *plan);
@@ -195,15 +201,32 @@ cudaError_t bc_lde_batch_plan_destroy(bc_lde_batch_plan *plan);
  * cudaFree: the schedule goes into a fixed 16 MiB array inside this library,
  * which every GPU that loads the library holds until the process exits.  A
  * batch whose schedule does not fit (about two million 4096-element work
- * items) returns cudaErrorInvalidValue.  The first call on a device looks up
- * the array's device address and the kernel's occupancy; make that first call
- * before any stream capture.  All calls on a device share the array: calls
+ * items) returns cudaErrorInvalidValue before its work items are built.  The
+ * first call on a device looks up the array's device address and the kernel's
+ * occupancy and keeps them for the life of the process: they do not survive
+ * cudaDeviceReset (or any other replacement of the device's primary context).
+ * The schedule is copied from host memory the call frees on return, so a call
+ * on a stream that is capturing returns cudaErrorStreamCaptureUnsupported and
+ * enqueues nothing.  All calls on a device share the array: calls
  * whose work overlaps on the GPU (different streams, not ordered by events)
  * race and corrupt each other; calls ordered on one stream are safe.
  * status (optional): if non-null, the call waits for the stream and stores
  * the batch status word (bit 0: a bounded dependency wait expired and the
  * outputs are invalid). */
 cudaError_t bc_lde_batch_noalloc(const bc_lde_job *jobs, uint32_t n_jobs, cudaStream_t stream, uint32_t *status);
+
+/* ---- the integer ceiling of the transform arithmetic ------------------------
+ * No counterpart in the reference.  Runs the transform kernels' radix-16 round
+ * arithmetic (a DIT round of 15 general multiplications plus the shift
+ * network, then a DIF round) on register-resident values in every resident
+ * thread slot of the device, `iters` times, with no memory traffic: its
+ * butterflies per second are the 32-bit integer issue roofline of the NTT
+ * kernels.  bc_butterfly_peak_words gives the size of `out` (the final values,
+ * written so that no arithmetic is dead); *butterflies receives the count the
+ * launch performs.  Asynchronous on `stream`; time it with events. */
+cudaError_t bc_butterfly_peak_words(size_t *out_words);
+cudaError_t bc_butterfly_peak(uint64_t *out, size_t out_words, uint32_t iters, cudaStream_t stream,
+                              uint64_t *butterflies);
 
 /* ---- continuous-batching LDE server ---------------------------------------
  * No counterpart in the reference.  One server per device: it creates the

@@ -136,3 +136,34 @@ def test_hybrid_plan_standalone_big_jobs(gpu_ctx):
             torch.cuda.synchronize()
             assert torch.equal(out, ref), f"min_ctas={min_ctas} log_n={log_n} cols={cols}"
         plan.close()
+
+
+def test_batch_wait_limit_expires_then_recovers(gpu_ctx):
+    """Failure detection of the persistent kernel's dependency waits, without a GPU fault.
+
+    One job of three dependent kernels, the first of them thousands of CTAs wide: the first work item of the
+    second kernel is taken while items of the first are still running, so it must wait.  With a wait limit of
+    one SM clock cycle that wait runs out: the kernel must set status bit 0, skip the item and still return
+    (the status read synchronises the stream).  With the default limit restored, the next run must be exact."""
+    import bc_ntt
+    import torch
+
+    rng = np.random.default_rng(99)
+    jobs = _mixed_jobs(rng, [(20, 64, 1)])
+    plan = bc_ntt.LdeBatch([j[:5] for j in jobs])
+    assert plan.info()["records"] >= 3
+    plan.set_wait_limit(1)
+    plan.run()
+    assert plan.status() & 1, "a one-cycle dependency wait must run out"
+    torch.cuda.synchronize()
+    plan.set_wait_limit(0)
+    for j in jobs:
+        j[1].fill_(0)
+    plan.run()
+    assert plan.status() == 0
+    ev, out, log_n, cols, log_b, _ = jobs[0]
+    ref = torch.empty_like(out)
+    bc_ntt.lde(ev, ref, log_n, cols, log_b, fused=True)
+    torch.cuda.synchronize()
+    assert torch.equal(out, ref)
+    plan.close()

@@ -40,3 +40,16 @@ def test_percentile():
     assert bench.pct(xs, 50) == 50
     assert bench.pct(xs, 99) == 99
     assert bench.pct([3.0], 99) == 3.0
+
+
+def test_uniform_words_in_field_and_seeded():
+    import numpy as np
+
+    a = bench.uniform_words(200_000, 5, device="cpu").numpy().view(np.uint64)
+    b = bench.uniform_words(200_000, 5, device="cpu").numpy().view(np.uint64)
+    assert np.array_equal(a, b)
+    assert (a < bench.P).all()
+    # both halves spread over their whole range (no fold onto small values)
+    hi, lo = a >> np.uint64(32), a & np.uint64(0xFFFFFFFF)
+    assert hi.max() > 0xFFF00000 and lo.max() > 0xFFF00000 and hi.min() < 0x100000
+    assert abs(float(hi.mean()) / 2**32 - 0.5) < 0.01

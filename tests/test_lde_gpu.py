@@ -61,6 +61,29 @@ def test_lde_large_sizes(gpu_ctx, log_n, cols, log_b):
         np.testing.assert_array_equal(run_lde(x, log_n, cols, log_b, fused), exp)
 
 
+def test_lde_large_config_two_whole_columns(gpu_ctx):
+    """The large configuration at full size -- 64 columns x 2^23, blowup 4 (16 GiB out) -- with two whole
+    columns (every coset, every position) checked against the oracle, through the fused and the plain path."""
+    import bc_ntt
+    import torch
+
+    log_n, cols, log_b = 23, 64, 2
+    n, B = 1 << log_n, 1 << log_b
+    g = torch.Generator(device="cuda").manual_seed(2023)
+    x = torch.randint(-(2**63), 2**63 - 1, (cols * n,), device="cuda", dtype=torch.int64, generator=g)
+    picks = [0, 37]
+    xs = np.concatenate([to_host(x[j * n:(j + 1) * n]) for j in picks])
+    exp = oracle.lde(xs, log_n, len(picks), n, log_b, threads=2).reshape(B, len(picks), n)
+    out = torch.empty(B * cols * n, dtype=torch.int64, device="cuda")
+    for fused in (True, False):
+        out.fill_(0)
+        bc_ntt.lde(x, out, log_n, cols, log_b, fused=fused)
+        torch.cuda.synchronize()
+        got = to_host(out.view(B, cols, n)[:, picks].contiguous())
+        np.testing.assert_array_equal(got, exp, err_msg=f"fused={fused}")
+    del x, out
+
+
 @pytest.mark.parametrize("log_n", [5, 12, 13, 18])
 def test_lde_column_major_and_strides(gpu_ctx, log_n):
     rng = np.random.default_rng(77 + log_n)

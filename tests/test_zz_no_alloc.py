@@ -85,3 +85,23 @@ def test_noalloc_batch_rejects_oversized_schedule(gpu_ctx):
     rc = bc_ntt.lib().bc_lde_batch_noalloc(ctypes.cast(big, ctypes.c_void_p), 1,
                                            torch.cuda.current_stream().cuda_stream, None)
     assert rc == 1  # cudaErrorInvalidValue
+
+
+def test_noalloc_batch_rejects_stream_capture(gpu_ctx):
+    """Its schedule is copied from host memory the call frees on return, so a call on a capturing stream is
+    refused (cudaErrorStreamCaptureUnsupported) and enqueues nothing; the stream stays usable afterwards."""
+    import torch
+
+    import bc_ntt
+
+    rng = np.random.default_rng(7)
+    jobs, arr = _jobs(rng, [(12, 2, 1)])
+    side = torch.cuda.Stream()
+    graph = torch.cuda.CUDAGraph()
+    rcs = []
+    with torch.cuda.graph(graph, stream=side):
+        rcs.append(bc_ntt.lib().bc_lde_batch_noalloc(ctypes.cast(arr, ctypes.c_void_p), 1, side.cuda_stream, None))
+    assert rcs == [900]  # cudaErrorStreamCaptureUnsupported
+    del graph
+    _run_noalloc(arr, 1)
+    _check_against_fused(jobs)
