@@ -349,8 +349,9 @@ class LdeServer:
 
 
 def autotune(log_n: int, log_blowup: int, num_cols: int, reps: int = 3) -> str:
-    """Times every candidate plan for (log_n, log_blowup) on the current device and keeps the fastest."""
-    buf = ctypes.create_string_buffer(8192)
+    """Times every candidate plan for (log_n, log_blowup) on the current device, then the launch knobs of the
+    best window split, and keeps the fastest; returns one report line per timed candidate."""
+    buf = ctypes.create_string_buffer(16384)
     _check(lib().bc_autotune(log_n, log_blowup, num_cols, reps, buf, len(buf)), "bc_autotune")
     return buf.value.decode()
 

@@ -132,7 +132,7 @@ bool lde_args_ok(uint32_t log_n, uint32_t num_cols, uint64_t stride_in, uint64_t
 
 bool build_lde_steps(const Plan &pl, const uint64_t *in, uint64_t *out, uint32_t log_n, uint32_t num_cols,
                      uint64_t stride_in, uint64_t stride_out, uint64_t coset_stride, uint32_t log_blowup,
-                     bool full_tile, int cols_factor_max, std::vector<LdeStep> &steps) {
+                     bool full_tile, int pass_walk, int top_walk, std::vector<LdeStep> &steps) {
   const DevTables *tabs = device_tables();
   if (!tabs) return false;
   steps.clear();
@@ -160,7 +160,8 @@ bool build_lde_steps(const Plan &pl, const uint64_t *in, uint64_t *out, uint32_t
     st.K = q.K;
     st.C = q.C;
     st.b2n = true;
-    if (!build_pass(q, cols_factor_max, st.pass, st.grid, st.threads, st.smem)) return false;
+    st.occ = pl.knobs.occ;
+    if (!build_pass(q, pass_walk, st.pass, st.grid, st.threads, st.smem)) return false;
     steps.push_back(st);
   }
   // B: top window
@@ -187,8 +188,7 @@ bool build_lde_steps(const Plan &pl, const uint64_t *in, uint64_t *out, uint32_t
     const uint64_t chunks = (num_cols + G - 1) / G;
     uint64_t factor = (tiles * chunks) / ((uint64_t)sm_count() * 8);
     if (factor < 1) factor = 1;
-    if (factor > (uint64_t)cols_factor_max) factor = cols_factor_max;
-    if (factor > (uint64_t)BC_TOP_COLS_FACTOR_MAX) factor = BC_TOP_COLS_FACTOR_MAX;
+    if (factor > (uint64_t)top_walk) factor = top_walk;
     p.cols_per_cta = G * (uint32_t)factor;
     p.canon_out = np == 1;
     p.vec_in = ((uintptr_t)p.in % 16 == 0 && p.stride_in % 2 == 0) ? 1 : 0;
@@ -205,10 +205,17 @@ bool build_lde_steps(const Plan &pl, const uint64_t *in, uint64_t *out, uint32_t
       return (size_t)top_smem_words(tile, K, tables) * sizeof(uint64_t) <= TOP_RESIDENT_SMEM_MAX;
     };
     uint32_t slots = 1;
-    if (fits(nb)) {
+    const bool can_prefetch = p.fwd_tables && K >= 4 && fits(2);
+    const uint8_t mode = pl.knobs.top_mode;
+    if (mode == TOP_MODE_REFILL) {
+      p.fwd_mode = TOP_TABLES_REFILL;
+    } else if (mode == TOP_MODE_PREFETCH && can_prefetch) {
+      p.fwd_mode = TOP_TABLES_PREFETCH;
+      slots = 2;
+    } else if (fits(nb)) {
       p.fwd_mode = TOP_TABLES_RESIDENT;
       slots = nb;
-    } else if (p.fwd_tables && K >= 4 && fits(2)) {
+    } else if (can_prefetch) {
       p.fwd_mode = TOP_TABLES_PREFETCH;
       slots = 2;
     } else {
@@ -221,8 +228,11 @@ bool build_lde_steps(const Plan &pl, const uint64_t *in, uint64_t *out, uint32_t
     const size_t smem1 = (size_t)top_smem_words(tile, K, slots, 1) * sizeof(uint64_t);
     const size_t smem2 = (size_t)top_smem_words(tile, K, slots, 2) * sizeof(uint64_t);
     p.dbuf = 0;
-    if (C == 8 && (uint32_t)K * nb <= 16 && p.fwd_mode != TOP_TABLES_PREFETCH && p.cols_per_cta > G &&
-        smem2 <= TOP_RESIDENT_SMEM_MAX) {
+    const bool dbuf_allowed = C == 8 && p.fwd_mode != TOP_TABLES_PREFETCH && p.cols_per_cta > G &&
+                              smem2 <= TOP_RESIDENT_SMEM_MAX;
+    if (pl.knobs.top_dbuf == 2) {
+      p.dbuf = dbuf_allowed ? 1 : 0;
+    } else if (pl.knobs.top_dbuf == 0 && dbuf_allowed && (uint32_t)K * nb <= 16) {
       const int n2 = top_ctas_per_sm(K, C, st.threads, smem2);
       p.dbuf = (n2 > 0 && n2 >= top_ctas_per_sm(K, C, st.threads, smem1)) ? 1 : 0;
     }
@@ -254,7 +264,8 @@ bool build_lde_steps(const Plan &pl, const uint64_t *in, uint64_t *out, uint32_t
     LdeStep st;
     st.K = q.K;
     st.C = q.C;
-    if (!build_pass(q, cols_factor_max, st.pass, st.grid, st.threads, st.smem)) return false;
+    st.occ = pl.knobs.occ;
+    if (!build_pass(q, pass_walk, st.pass, st.grid, st.threads, st.smem)) return false;
     steps.push_back(st);
   }
   return true;
@@ -270,7 +281,7 @@ cudaError_t launch_lde_step(const LdeStep &st, cudaStream_t stream) {
     }
     kern<<<st.grid, st.threads, st.smem, stream>>>(st.topp);
   } else {
-    PassKernel kern = pick_pass_kernel(st.K, st.C, st.b2n, st.pass.inverse != 0);
+    PassKernel kern = pick_pass_kernel(st.K, st.C, st.b2n, st.pass.inverse != 0, st.occ);
     if (!kern) return cudaErrorInvalidValue;
     if (st.smem > 48 * 1024) {
       cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)st.smem);
@@ -288,7 +299,7 @@ cudaError_t lde_fused(const Plan &pl, const uint64_t *in, uint64_t *out, uint32_
   if (num_cols == 0) return cudaSuccess;
   std::vector<LdeStep> steps;
   if (!build_lde_steps(pl, in, out, log_n, num_cols, stride_in, stride_out, coset_stride, log_blowup, false,
-                       BC_COLS_FACTOR_MAX, steps))
+                       plan_walk(pl), plan_top_walk(pl), steps))
     return cudaErrorInvalidConfiguration;
   uint32_t ev_used = 0;
   if (ev_used < n_ev) cudaEventRecord(ev[ev_used++], stream);

@@ -393,6 +393,7 @@ struct LdeStep {
   bool top = false;
   int K = 0, C = 1;
   bool b2n = false;
+  int occ = 0; // occupancy variant of a pass kernel (Knobs::occ)
   PassParams pass{};
   LdeTopParams topp{};
   dim3 grid;
@@ -402,10 +403,12 @@ struct LdeStep {
 
 // Steps of one fused LDE (inverse passes below the top window, the top-window
 // kernel, forward passes below it).  full_tile: 4096-element tiles (256
-// threads) for every step; cols_factor_max: column groups per CTA.
+// threads) for every step; pass_walk / top_walk: column groups a pass CTA /
+// a top-window CTA walks at most.  The plan's other knobs (top-window table
+// mode, double-buffering, pass occupancy) apply where the kernel allows them.
 bool build_lde_steps(const Plan &pl, const uint64_t *in, uint64_t *out, uint32_t log_n, uint32_t num_cols,
                      uint64_t stride_in, uint64_t stride_out, uint64_t coset_stride, uint32_t log_blowup,
-                     bool full_tile, int cols_factor_max, std::vector<LdeStep> &steps);
+                     bool full_tile, int pass_walk, int top_walk, std::vector<LdeStep> &steps);
 
 bool lde_args_ok(uint32_t log_n, uint32_t num_cols, uint64_t stride_in, uint64_t stride_out, uint64_t coset_stride,
                  uint32_t log_blowup);

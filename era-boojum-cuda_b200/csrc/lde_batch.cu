@@ -226,7 +226,7 @@ cudaError_t schedule(const bc_lde_job *jobs, uint32_t n_jobs, std::vector<BatchR
     if (standalone_min_ctas && standalone && jb.num_cols) {
       std::vector<LdeStep> own;
       if (!build_lde_steps(tuned_plan(jb.log_n, jb.log_blowup), jb.evals_bitrev, jb.out, jb.log_n, jb.num_cols,
-                           jb.stride_in, jb.stride_out, jb.coset_stride, jb.log_blowup, false, 8, own))
+                           jb.stride_in, jb.stride_out, jb.coset_stride, jb.log_blowup, false, 8, 8, own))
         return cudaErrorInvalidConfiguration;
       uint64_t min_ctas = ~0ull;
       for (const LdeStep &st : own) min_ctas = std::min<uint64_t>(min_ctas, (uint64_t)st.grid.x * st.grid.y);
@@ -238,7 +238,7 @@ cudaError_t schedule(const bc_lde_job *jobs, uint32_t n_jobs, std::vector<BatchR
     // the tuned plan, or the built-in one when the tuned plan uses a window shape this kernel does not carry
     auto build = [&](const Plan &pl) {
       if (!build_lde_steps(pl, jb.evals_bitrev, jb.out, jb.log_n, jb.num_cols, jb.stride_in, jb.stride_out,
-                           jb.coset_stride, jb.log_blowup, true, 4, steps[j]))
+                           jb.coset_stride, jb.log_blowup, true, 4, 4, steps[j]))
         return false;
       for (const LdeStep &st : steps[j])
         if (!batch_shape_supported(shape_id(st.top, st.b2n, st.K, st.C)) || st.threads != BATCH_THREADS ||

@@ -314,7 +314,27 @@ template <bool B2N, bool INV> static PassKernel pick(int K, int C) {
   return nullptr;
 }
 
-PassKernel pick_pass_kernel(int K, int C, bool b2n, bool inverse) {
+// The other occupancy variant of the C = 1 passes of 9..12 bits: 3 CTAs per SM
+// for natural->bit-reversed (default 2), 2 for bit-reversed->natural (default 3).
+template <bool B2N, bool INV> static PassKernel pick_occ(int K) {
+  constexpr int M = B2N ? BC_PASS_MIN_BLOCKS : BC_PASS_MIN_BLOCKS_B2N;
+  switch (K) {
+  case 9: return ntt_pass_kernel<9, 1, B2N, INV, M>;
+  case 10: return ntt_pass_kernel<10, 1, B2N, INV, M>;
+  case 11: return ntt_pass_kernel<11, 1, B2N, INV, M>;
+  case 12: return ntt_pass_kernel<12, 1, B2N, INV, M>;
+  default: return nullptr;
+  }
+}
+
+PassKernel pick_pass_kernel(int K, int C, bool b2n, bool inverse, int occ) {
+  const int dflt = (b2n && K >= 9) ? BC_PASS_MIN_BLOCKS_B2N : BC_PASS_MIN_BLOCKS;
+  if (occ && occ != dflt && C == 1 && K >= 9 && K <= 12) {
+    const int other = b2n ? BC_PASS_MIN_BLOCKS : BC_PASS_MIN_BLOCKS_B2N;
+    if (occ != other) return nullptr;
+    if (b2n) return inverse ? pick_occ<true, true>(K) : pick_occ<true, false>(K);
+    return inverse ? pick_occ<false, true>(K) : pick_occ<false, false>(K);
+  }
   if (b2n) return inverse ? pick<true, true>(K, C) : pick<true, false>(K, C);
   return inverse ? pick<false, true>(K, C) : pick<false, false>(K, C);
 }
@@ -401,8 +421,8 @@ cudaError_t launch_pass(const PassLaunch &pl, cudaStream_t stream) {
   dim3 grid;
   uint32_t threads;
   size_t smem;
-  if (!build_pass(pl, BC_COLS_FACTOR_MAX, p, grid, threads, smem)) return cudaErrorInvalidConfiguration;
-  PassKernel kern = pick_pass_kernel(pl.K, pl.C, pl.b2n, pl.inverse);
+  if (!build_pass(pl, pl.walk, p, grid, threads, smem)) return cudaErrorInvalidConfiguration;
+  PassKernel kern = pick_pass_kernel(pl.K, pl.C, pl.b2n, pl.inverse, pl.occ);
   if (!kern) return cudaErrorInvalidValue;
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -437,6 +457,8 @@ cudaError_t launch_ntt(const Plan &pl, const uint64_t *in, uint64_t *out, uint32
     q.canon_out = last;
     q.has_coset = log_ext > 0 ? 1 : 0;
     q.coset_kshift = coset_idx ? coset_idx << (PW_LOG - log_n - log_ext) : 0;
+    q.walk = plan_walk(pl);
+    q.occ = pl.knobs.occ;
     cudaError_t e = launch_pass(q, stream);
     if (e != cudaSuccess) return e;
   }

@@ -737,9 +737,11 @@ __host__ __device__ constexpr uint32_t pass_smem_words(uint32_t tile, int K) { r
 
 // One kernel per twiddle direction (INV == p.inverse, chosen on the host): a
 // kernel carrying both bodies behind a branch on p.inverse measured 4-10 us
-// slower per small launch in its second body.
-template <int K, int C, bool B2N, bool INV>
-__global__ void __launch_bounds__(256, (B2N && K >= 9) ? BC_PASS_MIN_BLOCKS_B2N : BC_PASS_MIN_BLOCKS)
+// slower per small launch in its second body.  MINB > 0 compiles the kernel for
+// MINB resident CTAs per SM instead of the default (the autotuner's occupancy
+// knob).
+template <int K, int C, bool B2N, bool INV, int MINB = 0>
+__global__ void __launch_bounds__(256, MINB ? MINB : ((B2N && K >= 9) ? BC_PASS_MIN_BLOCKS_B2N : BC_PASS_MIN_BLOCKS))
     ntt_pass_kernel(const PassParams p) {
   extern __shared__ uint64_t smem[];
   pass_body<K, C, B2N, INV>(p, blockIdx.x, blockIdx.y, smem);

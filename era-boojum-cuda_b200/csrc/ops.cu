@@ -60,51 +60,103 @@ __global__ void __launch_bounds__(OPS_THREADS) bitrev_swap_kernel(const uint64_t
   }
 }
 
+// Tile pair k of the triangle U <= V (k = V (V + 1) / 2 + U).
+__device__ __forceinline__ void decode_tile_pair(uint64_t k, uint32_t &U, uint32_t &V) {
+  uint64_t v = (uint64_t)((sqrtf(8.f * (float)k + 1.f) - 1.f) * 0.5f);
+  while ((v + 1) * (v + 2) / 2 <= k) v++;
+  while (v * (v + 1) / 2 > k) v--;
+  U = (uint32_t)(k - v * (v + 1) / 2);
+  V = (uint32_t)v;
+}
+
 // One CTA: tile pair blockIdx.x (triangular over U <= V), middle bit
-// blockIdx.z, columns blockIdx.y + k gridDim.y.
+// blockIdx.z, columns blockIdx.y + k gridDim.y.  VEC: 16-byte accesses -- a
+// warp moves two 32-element row segments per instruction (half-warps on
+// consecutive tile rows) and writes each destination row as pairs of
+// transposed elements; needs 16-byte aligned columns.  Measured on B200 (64
+// columns x 2^22, out of place): 0.644 ms against 0.685 ms with 8-byte
+// accesses and 0.667 ms for the reference's kernel.
+template <bool VEC>
 __global__ void __launch_bounds__(OPS_THREADS) bitrev_tile_kernel(const uint64_t *src, uint64_t ss, uint64_t *dst,
                                                                   uint64_t ds, uint32_t log_rows, uint32_t cols) {
   __shared__ uint64_t tile[2][32][33];
   const uint32_t h = log_rows >> 1, mbit = log_rows & 1;
-  const uint64_t k = blockIdx.x;
-  uint64_t V = (uint64_t)((sqrtf(8.f * (float)k + 1.f) - 1.f) * 0.5f);
-  while ((V + 1) * (V + 2) / 2 <= k) V++;
-  while (V * (V + 1) / 2 > k) V--;
-  const uint32_t U = (uint32_t)(k - V * (V + 1) / 2), Vv = (uint32_t)V;
+  uint32_t U, Vv;
+  decode_tile_pair(blockIdx.x, U, Vv);
   const uint32_t ntiles = U == Vv ? 1 : 2;
   const uint64_t mid = (uint64_t)blockIdx.z << h;
-  const uint32_t lane = threadIdx.x & 31, row0 = threadIdx.x >> 5; // 8 rows of 32 per pass
+  // 8-byte: lane = tile column, rows row0 + 8 j.  16-byte: lanes 0-15 / 16-31 of warp w on tile rows
+  // 2 (w + 8 j) and 2 (w + 8 j) + 1, two columns 2 l16, 2 l16 + 1 each.
+  const uint32_t lane = threadIdx.x & 31, row0 = threadIdx.x >> 5;
+  const uint32_t half = (threadIdx.x >> 4) & 1, l16 = threadIdx.x & 15;
   for (uint32_t col = blockIdx.y; col < cols; col += gridDim.y) {
     const uint64_t *s = src + (uint64_t)col * ss + mid;
     uint64_t *d = dst + (uint64_t)col * ds + mid;
-    uint64_t v[2][4];
+    if constexpr (VEC) {
+      ulonglong2 v[2][2];
 #pragma unroll
-    for (uint32_t q = 0; q < 2; q++) {
-      if (q < ntiles) {
-        const uint32_t tu = q ? Vv : U, tv = q ? U : Vv;
+      for (uint32_t q = 0; q < 2; q++) {
+        if (q < ntiles) {
+          const uint32_t tu = q ? Vv : U, tv = q ? U : Vv;
 #pragma unroll
-        for (uint32_t j = 0; j < 4; j++) {
-          const uint32_t t = row0 + 8 * j;
-          const uint64_t a = brev_n(32 * tu + t, h);
-          v[q][j] = __ldcs(s + (a << (h + mbit)) + 32 * tv + lane);
+          for (uint32_t j = 0; j < 2; j++) {
+            const uint64_t a = brev_n(32 * tu + 2 * (row0 + 8 * j) + half, h);
+            v[q][j] = __ldcs(reinterpret_cast<const ulonglong2 *>(s + (a << (h + mbit)) + 32 * tv) + l16);
+          }
         }
       }
-    }
 #pragma unroll
-    for (uint32_t q = 0; q < 2; q++)
-      if (q < ntiles)
+      for (uint32_t q = 0; q < 2; q++)
+        if (q < ntiles)
 #pragma unroll
-        for (uint32_t j = 0; j < 4; j++) tile[q][row0 + 8 * j][lane] = v[q][j];
-    __syncthreads();
+          for (uint32_t j = 0; j < 2; j++) {
+            const uint32_t t = 2 * (row0 + 8 * j) + half;
+            tile[q][t][2 * l16] = v[q][j].x;
+            tile[q][t][2 * l16 + 1] = v[q][j].y;
+          }
+      __syncthreads();
 #pragma unroll
-    for (uint32_t q = 0; q < 2; q++) {
-      if (q < ntiles) {
-        const uint32_t tu = q ? Vv : U, tv = q ? U : Vv;
+      for (uint32_t q = 0; q < 2; q++) {
+        if (q < ntiles) {
+          const uint32_t tu = q ? Vv : U, tv = q ? U : Vv;
 #pragma unroll
-        for (uint32_t j = 0; j < 4; j++) {
-          const uint32_t sidx = row0 + 8 * j; // column of the source tile = destination row
-          const uint64_t r = brev_n(32 * tv + sidx, h);
-          __stcs(d + (r << (h + mbit)) + 32 * tu + lane, tile[q][lane][sidx]);
+          for (uint32_t j = 0; j < 2; j++) {
+            const uint32_t sidx = 2 * (row0 + 8 * j) + half; // column of the source tile = destination row
+            const uint64_t r = brev_n(32 * tv + sidx, h);
+            __stcs(reinterpret_cast<ulonglong2 *>(d + (r << (h + mbit)) + 32 * tu) + l16,
+                   make_ulonglong2(tile[q][2 * l16][sidx], tile[q][2 * l16 + 1][sidx]));
+          }
+        }
+      }
+    } else {
+      uint64_t v[2][4];
+#pragma unroll
+      for (uint32_t q = 0; q < 2; q++) {
+        if (q < ntiles) {
+          const uint32_t tu = q ? Vv : U, tv = q ? U : Vv;
+#pragma unroll
+          for (uint32_t j = 0; j < 4; j++) {
+            const uint64_t a = brev_n(32 * tu + row0 + 8 * j, h);
+            v[q][j] = __ldcs(s + (a << (h + mbit)) + 32 * tv + lane);
+          }
+        }
+      }
+#pragma unroll
+      for (uint32_t q = 0; q < 2; q++)
+        if (q < ntiles)
+#pragma unroll
+          for (uint32_t j = 0; j < 4; j++) tile[q][row0 + 8 * j][lane] = v[q][j];
+      __syncthreads();
+#pragma unroll
+      for (uint32_t q = 0; q < 2; q++) {
+        if (q < ntiles) {
+          const uint32_t tu = q ? Vv : U, tv = q ? U : Vv;
+#pragma unroll
+          for (uint32_t j = 0; j < 4; j++) {
+            const uint32_t sidx = row0 + 8 * j; // column of the source tile = destination row
+            const uint64_t r = brev_n(32 * tv + sidx, h);
+            __stcs(d + (r << (h + mbit)) + 32 * tu + lane, tile[q][lane][sidx]);
+          }
         }
       }
     }
@@ -127,8 +179,12 @@ cudaError_t bit_reverse(const uint64_t *src, uint64_t ss, uint64_t *dst, uint64_
   } else {
     const uint64_t m = 1ull << ((log_rows >> 1) - 5);
     const uint64_t pairs = m * (m + 1) / 2;
-    bitrev_tile_kernel<<<dim3((uint32_t)pairs, gy, 1u << (log_rows & 1)), OPS_THREADS, 0, stream>>>(
-        src, ss, dst, ds, log_rows, cols);
+    const dim3 grid((uint32_t)pairs, gy, 1u << (log_rows & 1));
+    const bool vec = (uintptr_t)src % 16 == 0 && (uintptr_t)dst % 16 == 0 && (cols == 1 || (ss % 2 == 0 && ds % 2 == 0));
+    if (vec)
+      bitrev_tile_kernel<true><<<grid, OPS_THREADS, 0, stream>>>(src, ss, dst, ds, log_rows, cols);
+    else
+      bitrev_tile_kernel<false><<<grid, OPS_THREADS, 0, stream>>>(src, ss, dst, ds, log_rows, cols);
   }
   return cudaGetLastError();
 }

@@ -30,7 +30,7 @@ __device__ __forceinline__ uint64_t splitmix(uint64_t z) {
 // 64 butterflies per thread per iteration (one DIT and one DIF radix-16 round).
 // The powers are arbitrary canonical field elements of the thread; `out`
 // receives the 16 values so that no arithmetic is dead.
-__global__ void __launch_bounds__(PEAK_THREADS) butterfly_peak_kernel(uint64_t *out, uint32_t iters) {
+__global__ void __launch_bounds__(PEAK_THREADS, 2) butterfly_peak_kernel(uint64_t *out, uint32_t iters) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   uint64_t x[16], pd[15], pi[15];
 #pragma unroll

@@ -88,12 +88,18 @@ cudaError_t bc_batch_ntt_with_plan(const uint64_t *inputs, uint64_t *outputs, ui
  * the plain NTT; every entry point here uses the table's plan when present and
  * the built-in one otherwise.  bc_autotune times every candidate plan on the
  * current device (num_cols columns, reps timed runs after one warm-up; it
- * allocates and frees its own scratch and synchronises) and stores the
- * fastest; report (optional) receives one line per candidate. */
+ * allocates and frees its own scratch and synchronises), then the launch knobs
+ * of the fastest window split one at a time (column-group walk of the pass and
+ * top-window CTAs, top-window table mode and tile double-buffering, CTAs per
+ * SM of the low-window passes), and stores the fastest; report (optional)
+ * receives one line per timed candidate. */
 cudaError_t bc_autotune(uint32_t log_n, uint32_t log_blowup, uint32_t num_cols, uint32_t reps, char *report,
                         size_t report_len);
 /* Text form of the current device's table, one entry per line:
- * "log_n log_blowup npasses K0 C0 [K1 C1 [K2 C2]]" (passes from the top bits). */
+ * "log_n log_blowup npasses K0 C0 [K1 C1 [K2 C2]]" (passes from the top bits),
+ * followed by "k walk top_walk top_mode top_dbuf occ" when a launch knob is not
+ * the built-in choice (0 = built-in; top_mode 1 resident, 2 prefetched,
+ * 3 recomputed tables; top_dbuf 1 off, 2 on; occ 2 or 3 CTAs per SM). */
 cudaError_t bc_plan_table_export(char *buf, size_t len, size_t *needed);
 cudaError_t bc_plan_table_import(const char *text);
 cudaError_t bc_plan_table_clear(void);
