@@ -588,6 +588,7 @@ def run_ours(args, rank, world):
         line["large"] = run_large_section()
     if world == 1 and not args.no_serve:
         line["serve"] = run_serve_section()
+        line["serve_device"] = run_serve_device_section()
     if world == 1 and not args.no_ops:
         line["ops"] = run_ops_section(ops_ours(), log_n=args.ops_log_n)
     return line
@@ -1018,7 +1019,17 @@ def run_serve_section(n_requests: int = 24, rates=(10.0, 20.0), budget_gib: int 
                         "serial_plain_same_arrivals_p99_ms": round(pct(lat_serial, 99), 2)})
     st_cap = serve([0.0] * len(reqs))
     exact["capacity"] = exact_requests()
-    del hin, hout, expected
+    # the same requests device-resident (inputs and outputs in HBM, no PCIe): all queued at once
+    dev_in = [hin[o:o + r.in_words].to("cuda") for r, o in zip(reqs, in_off)]
+    dev_out = [torch.empty(r.out_words, dtype=torch.int64, device="cuda") for r in reqs]
+    device_mode = {}
+    for label, max_batch in (("coalesced", 1 << 22), ("per_request", 0)):
+        for t in dev_out:
+            t.zero_()
+        st_d, dst = serve_device(reqs, dev_in, dev_out, [0.0] * len(reqs), max_batch, budget_bytes=1 << 30)
+        device_mode[label] = {"value": round(st_d["out_melem_per_s"], 1), "span_s": round(st_d["span_s"], 4),
+                              **dst, "exact": sum(int(torch.equal(o, e)) for o, e in zip(dev_out, expected))}
+    del hin, hout, expected, dev_in, dev_out
     torch.cuda.empty_cache()
     return {"workload": f"{n_requests} requests, log_n U{{14..22}}, cols log-U[8,512], blowup U{{2,4}}, seed 7, "
                         f"per-request pinned host buffers, {budget_gib} GiB budget, {slots} slots",
@@ -1029,7 +1040,105 @@ def run_serve_section(n_requests: int = 24, rates=(10.0, 20.0), budget_gib: int 
             "capacity": {"server_value": round(st_cap["out_melem_per_s"], 1),
                          "serial_plain_value": round(out_elems / serial_s / 1e6, 1),
                          "speedup": round(st_cap["out_melem_per_s"] / (out_elems / serial_s / 1e6), 3),
-                         "server_span_s": round(st_cap["span_s"], 3), "serial_plain_s": round(serial_s, 3)}}
+                         "server_span_s": round(st_cap["span_s"], 3), "serial_plain_s": round(serial_s, 3)},
+            "device_resident_capacity": dict(device_mode, note="the same requests with inputs and outputs in device "
+                                             "memory (bc_lde_server_submit_device), all queued at once")}
+
+
+def serve_device(reqs, dev_in, dev_out, arrivals, max_batch_elems: int, budget_bytes: int = 1 << 30):
+    """Submits device-resident requests to a server at the given arrival times (seconds, paced by spinning on the
+    host clock), waits for all; returns (server stats, device-batching stats)."""
+    import bc_ntt
+
+    srv = bc_ntt.LdeServer(memory_budget_bytes=budget_bytes, slots=1)
+    srv.set_device_batching(max_batch_elems)
+    t0 = time.perf_counter()
+    ids = []
+    for r, a, o, at in zip(reqs, dev_in, dev_out, arrivals):
+        while time.perf_counter() - t0 < at:
+            pass
+        ids.append(srv.submit_device(a, o, r.log_n, r.cols, r.log_blowup))
+    for i in ids:
+        srv.wait(i, timeout_ms=600000)
+    st, dst = srv.stats(), srv.device_stats()
+    srv.close()
+    return st, dst
+
+
+def run_serve_device_section(n_requests: int = 300, rates=(5000.0, 20000.0)):
+    """Small LDE requests whose columns already sit in device memory (a prover's own earlier kernels produced
+    them): log_n U{10..16}, columns log-U[1,16], blowup U{2,4}, seeded Poisson arrivals.  The server coalesces
+    the device requests pending together into one persistent batch launch; against the same server running every
+    request as its own fused LDE, and against one fused call per request issued back to back on one stream (device
+    time).  Every request's output is checked against the same request alone after every run."""
+    import torch
+
+    import bc_ntt
+    import workloads
+
+    reqs = workloads.serving_stream(n_requests=n_requests, rate_per_s=rates[0], seed=9, log_n_range=(10, 16),
+                                    cols_range=(1, 16))
+    dev_in = [uniform_words(r.in_words, r.seed) for r in reqs]
+    dev_out = [torch.empty(r.out_words, dtype=torch.int64, device="cuda") for r in reqs]
+    expected = []
+    for r, a in zip(reqs, dev_in):
+        e = torch.empty(r.out_words, dtype=torch.int64, device="cuda")
+        bc_ntt.lde(a, e, r.log_n, r.cols, r.log_blowup, fused=True)
+        expected.append(e)
+    out_elems = sum(r.out_words for r in reqs)
+    stream = torch.cuda.current_stream()
+    # one fused call per request back to back on one stream: device time of each and in total
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(len(reqs) + 1)]
+    torch.cuda.synchronize()
+    evs[0].record(stream)
+    for i, (r, a, o) in enumerate(zip(reqs, dev_in, dev_out)):
+        bc_ntt.lde(a, o, r.log_n, r.cols, r.log_blowup, fused=True)
+        evs[i + 1].record(stream)
+    torch.cuda.synchronize()
+    service = [evs[i].elapsed_time(evs[i + 1]) for i in range(len(reqs))]
+    serial_ms = evs[0].elapsed_time(evs[-1])
+
+    def exact() -> int:
+        return sum(int(torch.equal(o, e)) for o, e in zip(dev_out, expected))
+
+    # first use of every kernel shape and of the server path (lazy module loading, attribute caches), untimed
+    for max_batch in (1 << 22, 0):
+        serve_device(reqs[:32], dev_in[:32], dev_out[:32], [0.0] * 32, max_batch)
+    res = {"workload": f"{n_requests} device-resident requests, log_n U{{10..16}}, cols log-U[1,16], blowup U{{2,4}}, "
+                       "seed 9", "unit": "Melem/s", "total_out_melem": round(out_elems / 1e6, 2),
+           "serial_fused_calls": {"value": round(out_elems / (serial_ms / 1e3) / 1e6, 1), "ms": round(serial_ms, 3),
+                                  "exact": exact()}}
+    for label, max_batch in (("coalesced", 1 << 22), ("per_request", 0)):
+        mode = {}
+        for t in dev_out:
+            t.zero_()
+        st, dst = serve_device(reqs, dev_in, dev_out, [0.0] * len(reqs), max_batch)
+        mode["capacity"] = {"value": round(st["out_melem_per_s"], 1), "span_ms": round(st["span_s"] * 1e3, 3),
+                            **dst, "exact": exact()}
+        for rate in rates:
+            arrivals = [r.arrival_s * rates[0] / rate for r in reqs]
+            for t in dev_out:
+                t.zero_()
+            st, dst = serve_device(reqs, dev_in, dev_out, arrivals, max_batch)
+            # FCFS one-at-a-time fused calls under the same arrivals, from their measured service times
+            t_free, lat = 0.0, []
+            for at, sv in zip(arrivals, service):
+                start = max(at * 1e3, t_free)
+                t_free = start + sv
+                lat.append(t_free - at * 1e3)
+            mode[f"rate_{rate:g}"] = {"p50_ms": round(st["p50_ms"], 3), "p99_ms": round(st["p99_ms"], 3),
+                                      **dst, "exact": exact(),
+                                      "serial_fused_same_arrivals_p50_ms": round(pct(lat, 50), 3),
+                                      "serial_fused_same_arrivals_p99_ms": round(pct(lat, 99), 3)}
+        res[label] = mode
+    runs = [res["serial_fused_calls"]["exact"]] + [m[k]["exact"] for m in (res["coalesced"], res["per_request"])
+                                                    for k in m]
+    res["bit_exact"] = all(v == len(reqs) for v in runs)
+    res["coalesced_vs_per_request_capacity"] = round(res["coalesced"]["capacity"]["value"] /
+                                                     max(res["per_request"]["capacity"]["value"], 1e-9), 3)
+    del dev_in, dev_out, expected
+    torch.cuda.empty_cache()
+    return res
 
 
 def run_reference(args, rank, world):

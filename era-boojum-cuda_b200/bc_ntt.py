@@ -71,6 +71,9 @@ SIGNATURES = {
     "bc_lde_batch_noalloc": [_vp, _u32, _vp, _vp],
     "bc_lde_server_create": [_vp, _vp],
     "bc_lde_server_submit": [_vp, _vp, _vp, _u32, _u32, _u32, _vp],
+    "bc_lde_server_submit_device": [_vp, _vp, _vp, _u32, _u32, _u32, _vp],
+    "bc_lde_server_set_device_batching": [_vp, _u64],
+    "bc_lde_server_get_device_stats": [_vp, _vp, _vp, _vp],
     "bc_lde_server_poll": [_vp, _u64, _vp, _vp],
     "bc_lde_server_wait": [_vp, _u64, _u32, _vp],
     "bc_lde_server_cancel": [_vp, _u64],
@@ -302,6 +305,24 @@ class LdeServer:
                                           ctypes.byref(rid)), "bc_lde_server_submit")
         self._keep[rid.value] = (host_evals, host_out)
         return rid.value
+
+    def submit_device(self, dev_evals, dev_out, log_n: int, num_cols: int, log_blowup: int) -> int:
+        """A request on device tensors (dense layouts); small pending ones are coalesced into one batch launch."""
+        rid = ctypes.c_uint64()
+        _check(lib().bc_lde_server_submit_device(self.handle, _ptr(dev_evals), _ptr(dev_out), log_n, num_cols,
+                                                 log_blowup, ctypes.byref(rid)), "bc_lde_server_submit_device")
+        self._keep[rid.value] = (dev_evals, dev_out)
+        return rid.value
+
+    def set_device_batching(self, max_batch_elems: int):
+        """Output elements up to which pending device requests are coalesced (0: none)."""
+        _check(lib().bc_lde_server_set_device_batching(self.handle, max_batch_elems), "set_device_batching")
+
+    def device_stats(self):
+        b, br, sr = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+        _check(lib().bc_lde_server_get_device_stats(self.handle, ctypes.byref(b), ctypes.byref(br), ctypes.byref(sr)),
+               "bc_lde_server_get_device_stats")
+        return {"batches": b.value, "batched_requests": br.value, "single_requests": sr.value}
 
     def poll(self, rid: int):
         st, lat = ctypes.c_int(), ctypes.c_double()

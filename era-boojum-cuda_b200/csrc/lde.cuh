@@ -8,6 +8,7 @@
 #include <cstdint>
 #include <vector>
 
+#include "../../include/bc_ntt.h"
 #include "ntt_host.cuh"
 #include "ntt_pass.cuh"
 
@@ -415,6 +416,12 @@ bool lde_args_ok(uint32_t log_n, uint32_t num_cols, uint64_t stride_in, uint64_t
 
 // Launches one step (pass or top-window kernel) on `stream`.
 cudaError_t launch_lde_step(const LdeStep &st, cudaStream_t stream);
+
+// Enqueues a batch of LDE jobs (bc_lde_job, include/bc_ntt.h) as one
+// persistent launch with its schedule in caller-owned device scratch, staged
+// through caller-owned pinned memory (lde_batch.cu).
+cudaError_t batch_enqueue_into(const bc_lde_job *jobs, uint32_t n_jobs, void *dev_scratch, void *host_staging,
+                               size_t scratch_bytes, cudaStream_t stream);
 
 // Launches the fused LDE's kernels on `stream`; events (optional): ev[0] is
 // recorded before the first kernel and ev[j + 1] after kernel j.

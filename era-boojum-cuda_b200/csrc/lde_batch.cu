@@ -23,6 +23,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <climits>
 #include <cstdint>
 #include <cstring>
@@ -174,11 +175,19 @@ uint32_t counter_words(uint32_t n_records) { return ((n_records + 2 + 1) & ~1u) 
 long long *wait_limit_slot(uint32_t *counters, uint32_t n_records) {
   return reinterpret_cast<long long *>(counters + counter_words(n_records) - 2);
 }
-// About 4 s of SM clock per dependency wait.
+// About 4 s of SM clock per dependency wait.  The clock-rate query costs
+// around a millisecond on some drivers, so it is made once per device.
 long long default_wait_limit(int device) {
+  static std::atomic<long long> cache[64];
+  if (device >= 0 && device < 64) {
+    const long long c = cache[device].load(std::memory_order_relaxed);
+    if (c) return c;
+  }
   int clock_khz = 0;
   cudaDeviceGetAttribute(&clock_khz, cudaDevAttrClockRate, device);
-  return (long long)std::max(clock_khz, 1000000) * 1000ll * 4;
+  const long long v = (long long)std::max(clock_khz, 1000000) * 1000ll * 4;
+  if (device >= 0 && device < 64) cache[device].store(v, std::memory_order_relaxed);
+  return v;
 }
 } // namespace
 
@@ -461,6 +470,61 @@ cudaError_t noalloc_setup(int dev, void **base, int *grid) {
   return cudaSuccess;
 }
 } // namespace
+} // namespace bc
+
+namespace bc {
+// Enqueues a batch on `stream` with its schedule in device scratch the caller
+// owns (used by the serving loop): the counters, records and items are
+// written into host_staging (pinned, at least scratch_bytes) and copied to
+// dev_scratch with one copy, then the persistent kernel runs.  The caller
+// must not reuse host_staging until that copy has completed, nor dev_scratch
+// until the kernel has.  A batch whose schedule exceeds scratch_bytes returns
+// cudaErrorInvalidValue before anything is enqueued.
+cudaError_t batch_enqueue_into(const bc_lde_job *jobs, uint32_t n_jobs, void *dev_scratch, void *host_staging,
+                               size_t scratch_bytes, cudaStream_t stream) {
+  if (n_jobs && !jobs) return cudaErrorInvalidValue;
+  if (!dev_scratch || !host_staging || (uintptr_t)dev_scratch % 256 || (uintptr_t)host_staging % 256)
+    return cudaErrorInvalidValue;
+  std::vector<BatchRecord> recs;
+  std::vector<uint64_t> items;
+  cudaError_t e = schedule(jobs, n_jobs, recs, items, 0, nullptr, scratch_bytes);
+  if (e != cudaSuccess) return e;
+  if (items.empty()) return cudaSuccess;
+  const uint32_t n_rec = (uint32_t)recs.size();
+  const size_t counters_bytes = round256(counter_words(n_rec) * sizeof(uint32_t));
+  const size_t recs_bytes = round256(recs.size() * sizeof(BatchRecord));
+  const size_t items_bytes = items.size() * sizeof(uint64_t);
+  const size_t total = counters_bytes + recs_bytes + items_bytes;
+  if (total > scratch_bytes) return cudaErrorInvalidValue;
+  unsigned char *h = static_cast<unsigned char *>(host_staging);
+  std::memset(h, 0, counters_bytes);
+  const long long limit = default_wait_limit(current_device());
+  std::memcpy(wait_limit_slot(reinterpret_cast<uint32_t *>(h), n_rec), &limit, sizeof(limit));
+  std::memcpy(h + counters_bytes, recs.data(), recs.size() * sizeof(BatchRecord));
+  std::memcpy(h + counters_bytes + recs_bytes, items.data(), items_bytes);
+  e = cudaMemcpyAsync(dev_scratch, host_staging, total, cudaMemcpyHostToDevice, stream);
+  if (e != cudaSuccess) return e;
+  static std::atomic<int> grid_cache[64];
+  const int dev = current_device();
+  int grid = (dev >= 0 && dev < 64) ? grid_cache[dev].load(std::memory_order_relaxed) : 0;
+  if (!grid) {
+    e = cudaFuncSetAttribute(lde_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)BATCH_SMEM_BYTES);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lde_batch_kernel, BATCH_THREADS, BATCH_SMEM_BYTES);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    grid = per_sm * sm_count();
+    if (dev >= 0 && dev < 64) grid_cache[dev].store(grid, std::memory_order_relaxed);
+  }
+  unsigned char *d = static_cast<unsigned char *>(dev_scratch);
+  uint32_t *counters = reinterpret_cast<uint32_t *>(d);
+  lde_batch_kernel<<<grid, BATCH_THREADS, BATCH_SMEM_BYTES, stream>>>(
+      reinterpret_cast<const BatchRecord *>(d + counters_bytes),
+      reinterpret_cast<const uint64_t *>(d + counters_bytes + recs_bytes), (uint32_t)items.size(), counters,
+      counters + n_rec, counters + n_rec + 1, wait_limit_slot(counters, n_rec));
+  return cudaGetLastError();
+}
 } // namespace bc
 
 extern "C" cudaError_t bc_lde_batch_noalloc(const bc_lde_job *jobs, uint32_t n_jobs, cudaStream_t stream,

@@ -264,6 +264,23 @@ typedef struct bc_lde_server bc_lde_server;
 cudaError_t bc_lde_server_create(const bc_lde_server_config *cfg, bc_lde_server **server);
 cudaError_t bc_lde_server_submit(bc_lde_server *server, const uint64_t *host_evals_bitrev, uint64_t *host_out,
                                  uint32_t log_n, uint32_t num_cols, uint32_t log_blowup, uint64_t *request_id);
+/* A request whose columns and output are already in device memory (dense
+ * layouts as above), e.g. produced by earlier GPU work: no copies, no arena.
+ * Device requests pending at the same moment whose output has at most
+ * max_batch_elems elements (bc_lde_server_set_device_batching; default 2^22)
+ * run together as ONE persistent batch launch (the batch kernel of
+ * bc_lde_batch_*), larger ones as their own fused LDE, all on the server's
+ * device stream with at most two launches in flight, so arrivals during a
+ * launch join the next one.  The buffers must stay valid until the request is
+ * done. */
+cudaError_t bc_lde_server_submit_device(bc_lde_server *server, const uint64_t *dev_evals_bitrev, uint64_t *dev_out,
+                                        uint32_t log_n, uint32_t num_cols, uint32_t log_blowup, uint64_t *request_id);
+/* 0: no coalescing, every device request runs as its own fused LDE. */
+cudaError_t bc_lde_server_set_device_batching(bc_lde_server *server, uint64_t max_batch_elems);
+/* Batch launches made for device requests, the requests they carried, and the
+ * device requests run as their own fused LDE. */
+cudaError_t bc_lde_server_get_device_stats(bc_lde_server *server, uint64_t *batches, uint64_t *batched_requests,
+                                           uint64_t *single_requests);
 /* *state: 0 pending, 1 running, 2 done, 3 cancelled, 4 failed (the call returns the error). */
 cudaError_t bc_lde_server_poll(bc_lde_server *server, uint64_t request_id, int *state, double *latency_ms);
 /* Waits up to timeout_ms: cudaErrorTimeout if still unfinished, cudaErrorNotReady if cancelled. */

@@ -117,3 +117,39 @@ def test_server_cancel_and_timeout_paths(gpu_ctx):
     st = srv.stats()
     assert st["completed"] == 2 and st["pending"] == 0 and st["running"] == 0
     srv.close()
+
+
+@pytest.mark.parametrize("max_batch_elems", [1 << 22, 0])
+def test_server_device_requests_equal_alone(gpu_ctx, max_batch_elems):
+    """Requests on device buffers: small ones pending together are coalesced into one persistent batch launch
+    (or, with coalescing off, each runs as its own fused LDE), big ones run alone; every result equals the same
+    request computed alone, bit for bit, including when host requests are in the mix."""
+    import bc_ntt
+    import torch
+
+    rng = np.random.default_rng(505)
+    specs = [(10 + (i % 7), 1 + (i * 5) % 9, 1 + i % 3) for i in range(40)] + [(21, 6, 1), (19, 20, 2)]
+    srv = bc_ntt.LdeServer(memory_budget_bytes=2 << 30, slots=2)
+    srv.set_device_batching(max_batch_elems)
+    reqs = []
+    for log_n, cols, log_b in specs:
+        x = raw_u64(rng, cols << log_n)
+        out = torch.full((((1 << log_b) * cols) << log_n,), 7, dtype=torch.int64, device="cuda")
+        reqs.append((x, out, log_n, cols, log_b))
+    hx = raw_u64(rng, 8 << 16)
+    hout = _pinned(np.zeros(2 * 8 << 16, dtype=np.uint64))
+    ids = [srv.submit_device(to_dev(x), out, log_n, cols, log_b) for x, out, log_n, cols, log_b in reqs]
+    hid = srv.submit(_pinned(hx), hout, 16, 8, 1)
+    for i in ids + [hid]:
+        srv.wait(i, timeout_ms=120000)
+    st = srv.device_stats()
+    srv.close()
+    for x, out, log_n, cols, log_b in reqs:
+        np.testing.assert_array_equal(to_host(out), _alone(x, log_n, cols, log_b),
+                                      err_msg=f"log_n={log_n} cols={cols} B={1 << log_b}")
+    np.testing.assert_array_equal(hout.numpy().view(np.uint64), _alone(hx, 16, 8, 1))
+    assert st["batched_requests"] + st["single_requests"] == len(specs)
+    if max_batch_elems:
+        assert st["batches"] >= 1 and st["batched_requests"] >= 2
+    else:
+        assert st["batches"] == 0
