@@ -247,7 +247,7 @@ cudaError_t schedule(const bc_lde_job *jobs, uint32_t n_jobs, std::vector<BatchR
     // the tuned plan, or the built-in one when the tuned plan uses a window shape this kernel does not carry
     auto build = [&](const Plan &pl) {
       if (!build_lde_steps(pl, jb.evals_bitrev, jb.out, jb.log_n, jb.num_cols, jb.stride_in, jb.stride_out,
-                           jb.coset_stride, jb.log_blowup, true, 4, 4, steps[j]))
+                           jb.coset_stride, jb.log_blowup, true, 16, 16, steps[j]))
         return false;
       for (const LdeStep &st : steps[j])
         if (!batch_shape_supported(shape_id(st.top, st.b2n, st.K, st.C)) || st.threads != BATCH_THREADS ||
