@@ -525,7 +525,8 @@ def run_ours(args, rank, world):
                                f"resident thread slot, best of 5 launches of {peak_ms:.1f} ms, this run",
                 "peak_clocks": peak_clocks,
                 "alu_pipe_pct": alu_pct, "fma_pipe_pct": fma_pct,
-                "pipe_source": "ncu of the top-window kernel, profiles/lde_kernels_ncu_full_8cols_logn22_blowup2.md"}
+                "pipe_source": "ncu of the top-window kernel and of the round loop, "
+                               "profiles/int32_roofline_butterfly_peak_and_lde_kernels_8cols_logn22_blowup2.md"}
 
     # end to end through the C ABI with host buffers: bc_lde_host takes pinned host input and writes pinned
     # host output every step, overlapping chunked copy-in / transform / copy-out on three streams
