@@ -335,11 +335,12 @@ __device__ __forceinline__ void cnet(uint64_t (&x)[16]) {
   }
 }
 
-// x[OFF + j] *= pp[j - 1] for j = 1 .. 2^V - 1.
+// x[OFF + j] *= pp[j - 1] for j = 1 .. 2^V - 1 (independent products: the
+// multiply-add chain form, gl::mul_chain).
 template <int V, int OFF>
 __device__ __forceinline__ void mul_powers(uint64_t (&x)[16], const uint64_t *pp) {
 #pragma unroll
-  for (int j = 1; j < (1 << V); j++) x[OFF + j] = gl::mul(x[OFF + j], pp[j - 1]);
+  for (int j = 1; j < (1 << V); j++) x[OFF + j] = gl::mul_chain(x[OFF + j], pp[j - 1]);
 }
 
 // Entry of a DIT round: with scale, x[OFF + j] *= pp[j - 1] (the upper half
@@ -350,9 +351,9 @@ __device__ __forceinline__ void dit_prepare(uint64_t (&x)[16], const uint64_t *p
   constexpr int H = 1 << (V - 1);
   if (scale) {
 #pragma unroll
-    for (int j = 1; j < H; j++) x[OFF + j] = gl::mul(x[OFF + j], pp[j - 1]);
+    for (int j = 1; j < H; j++) x[OFF + j] = gl::mul_chain(x[OFF + j], pp[j - 1]);
 #pragma unroll
-    for (int j = H; j < 2 * H; j++) x[OFF + j] = gl::mul_canon(x[OFF + j], pp[j - 1]);
+    for (int j = H; j < 2 * H; j++) x[OFF + j] = gl::mul_chain_canon(x[OFF + j], pp[j - 1]);
   } else {
 #pragma unroll
     for (int j = H; j < 2 * H; j++) x[OFF + j] = gl::canon(x[OFF + j]);
