@@ -258,19 +258,19 @@ __device__ __forceinline__ uint64_t sub_bc(uint64_t a, uint64_t b) {
 // carry, s - 2^64 + EPS < h * EPS + EPS <= p - 1 is already canonical; without
 // one, s >= p exactly when s + EPS carries, and then s + EPS - 2^64 = s - p.
 // CANON selects that canonical result; otherwise the carry is folded back as
-// EPS and the result is only < 2^64.
+// EPS and the result is only < 2^64.  lo + h * EPS is one multiply-add pair
+// (mad.lo.cc / madc.hi.cc by 0xffffffff), which runs on the multiplier pipe
+// and leaves the integer ALU, the transforms' bound, to the carries.
 template <bool CANON>
 __device__ __forceinline__ uint64_t add_h_eps(uint64_t lo, uint32_t h) {
   uint64_t r;
   if constexpr (CANON) {
     asm("{\n\t"
-        ".reg .u32 l0, l1, u0, u1, v0, v1, c;\n\t"
+        ".reg .u32 l0, l1, v0, v1, c;\n\t"
         ".reg .pred q;\n\t"
         "mov.b64 {l0, l1}, %1;\n\t"
-        "sub.cc.u32 u0, 0, %2;\n\t"
-        "subc.u32 u1, %2, 0;\n\t"
-        "add.cc.u32 l0, l0, u0;\n\t"
-        "addc.cc.u32 l1, l1, u1;\n\t"
+        "mad.lo.cc.u32 l0, %2, 0xffffffff, l0;\n\t"
+        "madc.hi.cc.u32 l1, %2, 0xffffffff, l1;\n\t"
         "addc.u32 c, 0, 0;\n\t"
         "add.cc.u32 v0, l0, 0xffffffff;\n\t"
         "addc.cc.u32 v1, l1, 0;\n\t"
@@ -284,12 +284,10 @@ __device__ __forceinline__ uint64_t add_h_eps(uint64_t lo, uint32_t h) {
         : "l"(lo), "r"(h));
   } else {
     asm("{\n\t"
-        ".reg .u32 l0, l1, u0, u1, c;\n\t"
+        ".reg .u32 l0, l1, c;\n\t"
         "mov.b64 {l0, l1}, %1;\n\t"
-        "sub.cc.u32 u0, 0, %2;\n\t"
-        "subc.u32 u1, %2, 0;\n\t"
-        "add.cc.u32 l0, l0, u0;\n\t"
-        "addc.cc.u32 l1, l1, u1;\n\t"
+        "mad.lo.cc.u32 l0, %2, 0xffffffff, l0;\n\t"
+        "madc.hi.cc.u32 l1, %2, 0xffffffff, l1;\n\t"
         "addc.u32 c, 0, 0;\n\t"
         "neg.s32 c, c;\n\t"
         "add.cc.u32 l0, l0, c;\n\t"
@@ -308,8 +306,9 @@ __device__ __forceinline__ uint64_t add_h_eps(uint64_t lo, uint32_t h) {
 //     = v0 - v2 - v3 + (v1 + v2 - v4) 2^32        (2^64 = 2^32 - 1, 2^96 = -1)
 // of which at most three words are non-zero for a given E.
 //   E < 32:       v = lo + h EPS, lo = x << E (64 bits), h = x >> (64 - E);
-//   32 <= E < 64: (v1 + v2) 2^32 - (v2 + v3), s = E - 32;
-//   64 <= E < 96: (v2 - v4) 2^32 - (v2 + v3), s = E - 64.
+//   32 <= E < 64: v1 2^32 + v2 EPS - v3, s = E - 32;
+//   64 <= E < 96: v2 EPS - (v3 + v4 2^32), s = E - 64.
+// Each product by EPS is a 32-bit multiply(-add) on the multiplier pipe.
 // CANON: the result is reduced to [0, p).
 template <int E, bool CANON = false>
 __device__ __forceinline__ uint64_t mul_pow2(uint64_t x) {
@@ -321,16 +320,16 @@ __device__ __forceinline__ uint64_t mul_pow2(uint64_t x) {
     const uint64_t xs = x << s;
     const uint32_t v1 = (uint32_t)xs, v2 = (uint32_t)(xs >> 32), v3 = s ? (uint32_t)(x >> (64 - s)) : 0u;
     uint64_t r;
-    // S = v1 + v2 (carry c1: S 2^32 = S_lo 2^32 + c1 EPS), D = v2 + v3, r = S 2^32 - D
+    // T = v2 EPS + (v1 2^32 + EPS - v3) (carry c), v = T - EPS: subtract
+    // (1 - c) EPS, then EPS once more on a borrow (only when v1 = v2 = 0)
     asm("{\n\t"
-        ".reg .u32 sl, m1, dl, c2, r0, r1, b;\n\t"
-        "add.cc.u32 sl, %1, %2;\n\t"
-        "addc.u32 m1, 0, 0;\n\t"
-        "neg.s32 m1, m1;\n\t"
-        "add.cc.u32 dl, %2, %3;\n\t"
-        "addc.u32 c2, 0, 0;\n\t"
-        "sub.cc.u32 r0, m1, dl;\n\t"
-        "subc.cc.u32 r1, sl, c2;\n\t"
+        ".reg .u32 z, r0, r1, m, b;\n\t"
+        "not.b32 z, %3;\n\t"
+        "mad.lo.cc.u32 r0, %2, 0xffffffff, z;\n\t"
+        "madc.hi.cc.u32 r1, %2, 0xffffffff, %1;\n\t"
+        "addc.u32 m, 0xffffffff, 0;\n\t"
+        "sub.cc.u32 r0, r0, m;\n\t"
+        "subc.cc.u32 r1, r1, 0;\n\t"
         "subc.u32 b, 0, 0;\n\t"
         "sub.cc.u32 r0, r0, b;\n\t"
         "subc.u32 r1, r1, 0;\n\t"
@@ -341,27 +340,24 @@ __device__ __forceinline__ uint64_t mul_pow2(uint64_t x) {
     return CANON ? canon(r) : r;
   } else {
     constexpr int s = E - 64;
-    const uint64_t xs = x << s;
-    const uint32_t y0 = (uint32_t)xs, y1 = (uint32_t)(xs >> 32), y2 = s ? (uint32_t)(x >> (64 - s)) : 0u;
+    // v = y0 EPS - Y with y0 = (x << s) mod 2^32 and Y = x >> (32 - s); a borrow
+    // leaves 2^64 + v >= 2^63 and is folded back by subtracting EPS
+    const uint32_t y0 = (uint32_t)x << s;
+    const uint64_t t = (uint64_t)y0 * 0xffffffffull, Y = x >> (32 - s);
     uint64_t r;
-    // S = y0 - y2 (borrow: S 2^32 = S_lo 2^32 - EPS), D = y0 + y1 (+ EPS on that borrow), r = S_lo 2^32 - D
     asm("{\n\t"
-        ".reg .u32 sl, m, dl, dh, r0, r1, b;\n\t"
-        "sub.cc.u32 sl, %1, %3;\n\t"
-        "subc.u32 m, 0, 0;\n\t"
-        "add.cc.u32 dl, %1, %2;\n\t"
-        "addc.u32 dh, 0, 0;\n\t"
-        "add.cc.u32 dl, dl, m;\n\t"
-        "addc.u32 dh, dh, 0;\n\t"
-        "sub.cc.u32 r0, 0, dl;\n\t"
-        "subc.cc.u32 r1, sl, dh;\n\t"
+        ".reg .u32 t0, t1, y0, y1, r0, r1, b;\n\t"
+        "mov.b64 {t0, t1}, %1;\n\t"
+        "mov.b64 {y0, y1}, %2;\n\t"
+        "sub.cc.u32 r0, t0, y0;\n\t"
+        "subc.cc.u32 r1, t1, y1;\n\t"
         "subc.u32 b, 0, 0;\n\t"
         "sub.cc.u32 r0, r0, b;\n\t"
         "subc.u32 r1, r1, 0;\n\t"
         "mov.b64 %0, {r0, r1};\n\t"
         "}"
         : "=l"(r)
-        : "r"(y0), "r"(y1), "r"(y2));
+        : "l"(t), "l"(Y));
     return CANON ? canon(r) : r;
   }
 }
