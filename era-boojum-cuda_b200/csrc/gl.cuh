@@ -110,10 +110,11 @@ __device__ __forceinline__ uint64_t mul(uint64_t a, uint64_t b) { return reduce1
 // reduce128 with a canonical result: t0 = lo - hh is formed as there; for
 // s = t0 + hl * EPS, a carry out of 2^64 leaves s - 2^64 + EPS < p, and
 // without one s >= p exactly when s + EPS carries (then s + EPS - 2^64 = s - p).
+// hl * EPS goes in with one multiply-add pair (mad.lo.cc / madc.hi.cc).
 __device__ __forceinline__ uint64_t reduce128_canon(uint64_t lo, uint64_t hi) {
   uint64_t r;
   asm("{\n\t"
-      ".reg .u32 l0, l1, hl, hh, t0, t1, u0, u1, v0, v1, c;\n\t"
+      ".reg .u32 l0, l1, hl, hh, t0, t1, v0, v1, c;\n\t"
       ".reg .pred q;\n\t"
       "mov.b64 {l0, l1}, %1;\n\t"
       "mov.b64 {hl, hh}, %2;\n\t"
@@ -122,10 +123,8 @@ __device__ __forceinline__ uint64_t reduce128_canon(uint64_t lo, uint64_t hi) {
       "subc.u32 c, 0, 0;\n\t"
       "sub.cc.u32 t0, t0, c;\n\t"
       "subc.u32 t1, t1, 0;\n\t"
-      "sub.cc.u32 u0, 0, hl;\n\t"
-      "subc.u32 u1, hl, 0;\n\t"
-      "add.cc.u32 t0, t0, u0;\n\t"
-      "addc.cc.u32 t1, t1, u1;\n\t"
+      "mad.lo.cc.u32 t0, hl, 0xffffffff, t0;\n\t"
+      "madc.hi.cc.u32 t1, hl, 0xffffffff, t1;\n\t"
       "addc.u32 c, 0, 0;\n\t"
       "add.cc.u32 v0, t0, 0xffffffff;\n\t"
       "addc.cc.u32 v1, t1, 0;\n\t"
