@@ -237,6 +237,17 @@ bool build_lde_steps(const Plan &pl, const uint64_t *in, uint64_t *out, uint32_t
       p.dbuf = (n2 > 0 && n2 >= top_ctas_per_sm(K, C, st.threads, smem1)) ? 1 : 0;
     }
     st.smem = p.dbuf ? smem2 : smem1;
+    // the scale factors once per CTA in shared memory, when the CTA walks more
+    // than one column group and the table costs no resident CTA per SM
+    p.scale_off = 0;
+    if (K >= 4 && p.cols_per_cta > G) {
+      const size_t with = st.smem + (size_t)tile * sizeof(uint64_t);
+      if (with <= TOP_RESIDENT_SMEM_MAX &&
+          top_ctas_per_sm(K, C, st.threads, with) >= top_ctas_per_sm(K, C, st.threads, st.smem)) {
+        p.scale_off = (uint32_t)(st.smem / sizeof(uint64_t));
+        st.smem = with;
+      }
+    }
     const uint64_t gy = (num_cols + p.cols_per_cta - 1) / p.cols_per_cta;
     if (gy > 65535 || tiles > 0x7fffffffull) return false;
     st.grid = dim3((uint32_t)tiles, (uint32_t)gy);

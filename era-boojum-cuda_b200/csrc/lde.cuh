@@ -57,6 +57,9 @@ struct LdeTopParams {
   const uint64_t *inv_table;  // precomputed inverse table (or nullptr)
   uint32_t dbuf;              // two tiles, the next column group copied (cp.async) during this one;
                               // honoured by the 8-column kernels only (C == 8)
+  uint32_t scale_off;         // windows of 4 bits or more: word offset in shared memory of the
+                              // threads' scale factors n^-1 g^i (16 per thread, computed once per CTA
+                              // and reused by every column group it walks); 0: recomputed per group
   DevTables tabs;
 };
 
@@ -162,6 +165,28 @@ __device__ __forceinline__ void top_body(const LdeTopParams &p, uint32_t bx, uin
   // the column loop's first barrier orders these fills before any use
 
   const uint64_t inv_n = p.tabs.inv_pow2[p.log_n];
+
+  // scale n^-1 g^i of the inverse window's output: element j of the thread's
+  // group (after the last inverse round) has natural index
+  // i0 + (j << (lb + K - 4)), i0 = base_off + tid % C + (w << lb); one factor
+  // to start and 15 running products
+  auto scale_factors = [&](uint32_t w, auto &&use) {
+    const uint32_t i0 = (uint32_t)base_off + tid % C + (w << p.lb);
+    const uint64_t g_step = g_power(p.tabs, 0, 1u << (p.lb + K - 4));
+    uint64_t s = gl::mul(inv_n, g_power(p.tabs, 0, i0));
+#pragma unroll
+    for (int j = 0; j < 16; j++) {
+      use(j, s);
+      if (j + 1 < 16) s = gl::mul(s, g_step);
+    }
+  };
+  uint64_t *const scale_tab = (NF > 0 && p.scale_off) ? smem + p.scale_off : nullptr;
+  if (scale_tab) {
+    // each thread reads back only its own factors: no barrier needed
+    uint32_t w;
+    gbase16<K, C>(tid, K - 4, w);
+    scale_factors(w, [&](int j, uint64_t s) { scale_tab[j * T + tid] = s; });
+  }
 
   // the tile of column group c by loads and stores
   auto load_tile = [&](uint64_t *dst, uint32_t c) {
@@ -297,16 +322,12 @@ __device__ __forceinline__ void top_body(const LdeTopParams &p, uint32_t bx, uin
           for (int j = 0; j < 16; j++) coef[j] = x[j];
         }
       }
-      // scale n^-1 g^i: element j of this thread's group has natural index i0 + (j << (lb + K - 4))
-      {
-        const uint32_t i0 = (uint32_t)base_off + tid % C + (w << p.lb);
-        const uint64_t g_step = g_power(p.tabs, 0, 1u << (p.lb + K - 4));
-        uint64_t s = gl::mul(inv_n, g_power(p.tabs, 0, i0));
+      // scale n^-1 g^i
+      if (scale_tab) {
 #pragma unroll
-        for (int j = 0; j < 16; j++) {
-          coef[j] = gl::mul(coef[j], s);
-          if (j + 1 < 16) s = gl::mul(s, g_step);
-        }
+        for (int j = 0; j < 16; j++) coef[j] = gl::mul_chain(coef[j], scale_tab[j * T + tid]);
+      } else {
+        scale_factors(w, [&](int j, uint64_t s) { coef[j] = gl::mul(coef[j], s); });
       }
       for (uint32_t k = 0; k < nb; k++) {
         __syncthreads(); // previous coset's stores have read the tile (and the powers)
