@@ -308,7 +308,8 @@ __device__ __forceinline__ uint64_t add_h_eps(uint64_t lo, uint32_t h) {
 //   32 <= E < 64: v1 2^32 + v2 EPS - v3, s = E - 32;
 //   64 <= E < 96: v2 EPS - (v3 + v4 2^32), s = E - 64.
 // Each product by EPS is a 32-bit multiply(-add) on the multiplier pipe.
-// CANON: the result is reduced to [0, p).
+// CANON: the result is reduced to [0, p); for E >= 32 it always is (bounds at
+// each case), so only E < 32 pays for it.
 template <int E, bool CANON = false>
 __device__ __forceinline__ uint64_t mul_pow2(uint64_t x) {
   static_assert(E > 0 && E < 96, "mul_pow2: 0 < E < 96");
@@ -320,7 +321,9 @@ __device__ __forceinline__ uint64_t mul_pow2(uint64_t x) {
     const uint32_t v1 = (uint32_t)xs, v2 = (uint32_t)(xs >> 32), v3 = s ? (uint32_t)(x >> (64 - s)) : 0u;
     uint64_t r;
     // T = v2 EPS + (v1 2^32 + EPS - v3) (carry c), v = T - EPS: subtract
-    // (1 - c) EPS, then EPS once more on a borrow (only when v1 = v2 = 0)
+    // (1 - c) EPS, then EPS once more on a borrow (only when v1 = v2 = 0).
+    // Canonical: T < 2^65 - 2^33, so with c = 1 the result T - 2^64 < p; with
+    // c = 0, T - EPS <= p - 1, and after a borrow T - EPS + p is in [p - EPS, p).
     asm("{\n\t"
         ".reg .u32 z, r0, r1, m, b;\n\t"
         "not.b32 z, %3;\n\t"
@@ -336,11 +339,13 @@ __device__ __forceinline__ uint64_t mul_pow2(uint64_t x) {
         "}"
         : "=l"(r)
         : "r"(v1), "r"(v2), "r"(v3));
-    return CANON ? canon(r) : r;
+    return r;
   } else {
     constexpr int s = E - 64;
     // v = y0 EPS - Y with y0 = (x << s) mod 2^32 and Y = x >> (32 - s); a borrow
-    // leaves 2^64 + v >= 2^63 and is folded back by subtracting EPS
+    // leaves 2^64 + v >= 2^63 and is folded back by subtracting EPS.
+    // Canonical: y0 EPS <= p - 2^32, so without a borrow v < p, and after one
+    // v + p is in (p - 2^63, p).
     const uint32_t y0 = (uint32_t)x << s;
     const uint64_t t = (uint64_t)y0 * 0xffffffffull, Y = x >> (32 - s);
     uint64_t r;
@@ -357,7 +362,7 @@ __device__ __forceinline__ uint64_t mul_pow2(uint64_t x) {
         "}"
         : "=l"(r)
         : "l"(t), "l"(Y));
-    return CANON ? canon(r) : r;
+    return r;
   }
 }
 

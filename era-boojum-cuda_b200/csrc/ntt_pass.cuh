@@ -162,8 +162,8 @@ __device__ __forceinline__ uint32_t brev_bits(uint32_t x, uint32_t bits) { retur
 // R = 0 network followed by x_j <- x_j s^j.  The R = 0 network's twiddles
 // T[u], u < 8, are signed powers of two (small_tw_exp), applied with shifts
 // (gl::mul_pow2): a round costs 2^V - 1 general multiplications instead of
-// V 2^(V-1), plus shift multiplications.  A DIT butterfly by -2^e swaps its
-// sum and difference; a DIF one swaps the operands of its difference.
+// V 2^(V-1), plus shift multiplications.  Both networks use Cooley-Tukey
+// butterflies (cstage); one by -2^e swaps its sum and difference.
 //
 // Power table of one tile position.  The window's rounds partition its bits
 // into full rounds [K - 4(i+1), K - 4i) from the top and a short round
@@ -297,40 +297,40 @@ template <int E, bool BCAN = false> __device__ __forceinline__ void cdit(uint64_
   }
 }
 
-template <int E> __device__ __forceinline__ void cdif(uint64_t &a, uint64_t &b) {
-  const uint64_t a0 = a;
-  a = gl::add(a0, b);
-  if constexpr (E == 0)
-    b = gl::sub(a0, b);
-  else if constexpr (E < 96)
-    b = gl::mul_pow2<E>(gl::sub(a0, b));
-  else
-    b = gl::mul_pow2<E - 96>(gl::sub(b, a0));
-}
-
-// One stage (bit QQ of a V-bit round) of the R = 0 network on x[OFF .. OFF + 2^V).
+// One stage (pair bit QQ of a V-bit round) of the R = 0 network on
+// x[OFF .. OFF + 2^V), Cooley-Tukey butterflies (twiddle, then sum and
+// difference).  DIT network: stages top bit first, the pair's twiddle is T[u]
+// of the round bits u above QQ.  DIF network: stages bottom bit first, twiddle
+// w_{2^(QQ+1)}^(-+j) of the round bits j below QQ (ct_tw_exp).  The DIF
+// network, the stage-by-stage inverse of the DIT one with the other table,
+// is 2^V N_DIT^-1 = DFT(w^-+1) composed with the bit-reversal of its input,
+// and the in-place Cooley-Tukey iteration computes exactly that map on the
+// same registers; its butterflies (canonical shift product, one correction per
+// add and subtract) cost fewer instructions than sum-then-twiddle ones.
 // BCAN: the stage's second operands are canonical.
 template <bool DIF, bool INV, int V, int OFF, int QQ, bool BCAN, int J0 = 0>
 __device__ __forceinline__ void cstage(uint64_t (&x)[16]) {
   if constexpr (J0 < (1 << V)) {
     if constexpr (!(J0 & (1 << QQ))) {
-      constexpr int E = small_tw_exp(INV, J0 >> (QQ + 1));
-      if constexpr (DIF)
-        cdif<E>(x[OFF + J0], x[OFF + (J0 | (1 << QQ))]);
-      else
-        cdit<E, BCAN>(x[OFF + J0], x[OFF + (J0 | (1 << QQ))]);
+      constexpr int E = DIF ? ct_tw_exp(INV, QQ, J0 & ((1 << QQ) - 1)) : small_tw_exp(INV, J0 >> (QQ + 1));
+      cdit<E, BCAN>(x[OFF + J0], x[OFF + (J0 | (1 << QQ))]);
     }
     cstage<DIF, INV, V, OFF, QQ, BCAN, J0 + 1>(x);
   }
 }
 
 // The R = 0 network of a V-bit round: DIT top bit first, DIF bottom bit first.
-// DIT rounds enter with their upper half canonical (dit_prepare), so the
-// first stage -- all twiddles 1 -- takes one carry correction per add/sub.
+// Either way the first stage's twiddles are all 1: DIT rounds enter with their
+// upper half canonical (dit_prepare), DIF rounds reduce their odd elements
+// here, so that stage takes one carry correction per add and subtract.
 template <bool DIF, bool INV, int V, int OFF, int S = 0>
 __device__ __forceinline__ void cnet(uint64_t (&x)[16]) {
+  if constexpr (DIF && S == 0) {
+#pragma unroll
+    for (int j = 1; j < (1 << V); j += 2) x[OFF + j] = gl::canon(x[OFF + j]);
+  }
   if constexpr (S < V) {
-    cstage<DIF, INV, V, OFF, DIF ? S : V - 1 - S, !DIF && S == 0>(x);
+    cstage<DIF, INV, V, OFF, DIF ? S : V - 1 - S, S == 0>(x);
     cnet<DIF, INV, V, OFF, S + 1>(x);
   }
 }

@@ -43,6 +43,14 @@ __host__ __device__ constexpr int small_tw_exp(bool inv, int u) {
   return inv ? (192 - fwd[u]) % 192 : fwd[u];
 }
 
+// Twiddle of the Cooley-Tukey form of a DIF round's network: the stage that
+// pairs round bit qq multiplies by w_{2^(qq+1)}^j (inverse: w^-j), j = the
+// round bits below qq; w_{2^(qq+1)} = w_16^(2^(3-qq)) = 2^(156 * 2^(3-qq)).
+__host__ __device__ constexpr int ct_tw_exp(bool inv, int qq, int j) {
+  const int e = (156 * (j << (3 - qq))) % 192;
+  return inv ? (192 - e) % 192 : e;
+}
+
 struct DevTables {
   const uint64_t *tw_lo[2]; // [0] forward, [1] inverse
   const uint64_t *tw_hi[2];
