@@ -252,31 +252,28 @@ __device__ __forceinline__ uint64_t sub_bc(uint64_t a, uint64_t b) {
   return r;
 }
 
-// lo + h * EPS (mod p) for h < 2^32.  h * EPS = (h << 32) - h <= 2^64 - 2^33 + 1
-// needs no reduction, and s = lo + h * EPS carries at most once.  After a
-// carry, s - 2^64 + EPS < h * EPS + EPS <= p - 1 is already canonical; without
-// one, s >= p exactly when s + EPS carries, and then s + EPS - 2^64 = s - p.
-// CANON selects that canonical result; otherwise the carry is folded back as
-// EPS and the result is only < 2^64.  lo + h * EPS is one multiply-add pair
-// (mad.lo.cc / madc.hi.cc by 0xffffffff), which runs on the multiplier pipe
-// and leaves the integer ALU, the transforms' bound, to the carries.
+// lo + h * EPS (mod p) for h < 2^32 (h < 2^32 - 1 for CANON).  h * EPS =
+// (h << 32) - h <= 2^64 - 2^33 + 1 needs no reduction, and s = lo + h * EPS
+// carries at most once; without CANON the carry is folded back as EPS and the
+// result is only < 2^64.  CANON forms s' = lo + (h + 1) * EPS = s + EPS < 2^65
+// instead: s' carries exactly when s >= p, and then s' - 2^64 = s - p;
+// without a carry the result is s' - EPS = s < p.  Either way lo + h * EPS is
+// one multiply-add pair (mad.lo.cc / madc.hi.cc by 0xffffffff), which runs on
+// the multiplier pipe and leaves the integer ALU, the transforms' bound, to
+// the carries.
 template <bool CANON>
 __device__ __forceinline__ uint64_t add_h_eps(uint64_t lo, uint32_t h) {
   uint64_t r;
   if constexpr (CANON) {
     asm("{\n\t"
-        ".reg .u32 l0, l1, v0, v1, c;\n\t"
-        ".reg .pred q;\n\t"
+        ".reg .u32 l0, l1, h1, m;\n\t"
         "mov.b64 {l0, l1}, %1;\n\t"
-        "mad.lo.cc.u32 l0, %2, 0xffffffff, l0;\n\t"
-        "madc.hi.cc.u32 l1, %2, 0xffffffff, l1;\n\t"
-        "addc.u32 c, 0, 0;\n\t"
-        "add.cc.u32 v0, l0, 0xffffffff;\n\t"
-        "addc.cc.u32 v1, l1, 0;\n\t"
-        "addc.u32 c, c, 0;\n\t"
-        "setp.ne.u32 q, c, 0;\n\t"
-        "selp.b32 l0, v0, l0, q;\n\t"
-        "selp.b32 l1, v1, l1, q;\n\t"
+        "add.u32 h1, %2, 1;\n\t"
+        "mad.lo.cc.u32 l0, h1, 0xffffffff, l0;\n\t"
+        "madc.hi.cc.u32 l1, h1, 0xffffffff, l1;\n\t"
+        "addc.u32 m, 0xffffffff, 0;\n\t"
+        "sub.cc.u32 l0, l0, m;\n\t"
+        "subc.u32 l1, l1, 0;\n\t"
         "mov.b64 %0, {l0, l1};\n\t"
         "}"
         : "=l"(r)
