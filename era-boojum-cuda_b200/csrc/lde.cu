@@ -199,8 +199,9 @@ bool build_lde_steps(const Plan &pl, const uint64_t *in, uint64_t *out, uint32_t
     const uint32_t nb = 1u << log_blowup;
     // forward power tables: all resident if they fit with two CTAs per SM, else
     // two slots fed ahead by cp.async from the precomputed ones, else refilled
-    p.fwd_tables = top_power_tables((uint32_t)K, log_blowup, false);
-    p.inv_table = top_power_tables((uint32_t)K, log_blowup, true);
+    const bool direct = top_direct(K, C); // top_body_direct: short-round-on-top tables, one tile
+    p.fwd_tables = top_power_tables((uint32_t)K, log_blowup, false, direct);
+    p.inv_table = top_power_tables((uint32_t)K, log_blowup, true, direct);
     auto fits = [&](uint32_t tables) {
       return (size_t)top_smem_words(tile, K, tables) * sizeof(uint64_t) <= TOP_RESIDENT_SMEM_MAX;
     };
@@ -228,7 +229,7 @@ bool build_lde_steps(const Plan &pl, const uint64_t *in, uint64_t *out, uint32_t
     const size_t smem1 = (size_t)top_smem_words(tile, K, slots, 1) * sizeof(uint64_t);
     const size_t smem2 = (size_t)top_smem_words(tile, K, slots, 2) * sizeof(uint64_t);
     p.dbuf = 0;
-    const bool dbuf_allowed = C == 8 && p.fwd_mode != TOP_TABLES_PREFETCH && p.cols_per_cta > G &&
+    const bool dbuf_allowed = !direct && C == 8 && p.fwd_mode != TOP_TABLES_PREFETCH && p.cols_per_cta > G &&
                               smem2 <= TOP_RESIDENT_SMEM_MAX;
     if (pl.knobs.top_dbuf == 2) {
       p.dbuf = dbuf_allowed ? 1 : 0;

@@ -121,10 +121,231 @@ __device__ __forceinline__ void top_store_regs(const LdeTopParams &p, const uint
   }
 }
 
+// The top-window kernel takes its direct path (top_body_direct) for windows of
+// 4 bits or more over runs of C >= 4 low positions (a run fills a 32-byte
+// sector, so a warp's 8-byte accesses to one window position are whole
+// sectors); its power tables use the short-round-on-top partition
+// (ShortTopShape) when K mod 4 != 0.
+__host__ __device__ constexpr bool top_direct(int K, int C) { return K >= 4 && C >= 4; }
+
+// The top round of the direct path on every group of the thread: NV = 2^V
+// values per group, the same powers for all (R_local = 0).  DIT: with scale,
+// x_j *= pp[j - 1] first; DIF: no powers (the inverse top round has s = 1).
+template <bool DIF, bool INV, int V, int Q = 0>
+__device__ __forceinline__ void top_round_groups(uint64_t (&x)[16], const uint64_t *pp, bool scale) {
+  constexpr int NV = 1 << V;
+  if constexpr (Q < 16 / NV) {
+    if constexpr (!DIF) dit_prepare<V, Q * NV>(x, pp, scale);
+    cnet<DIF, INV, V, Q * NV>(x);
+    top_round_groups<DIF, INV, V, Q + 1>(x, pp, scale);
+  }
+}
+
+// Direct path of the top-window kernel (top_direct(K, C)).  The window's
+// rounds are the full rounds [0, 4), [4, 8), ... and on top a short round of
+// K mod 4 bits (or the last full round when K mod 4 = 0).  The inverse runs
+// them bottom-up: the bottom round is loaded straight from global memory into
+// registers (thread: 16 consecutive window positions of one low position;
+// C consecutive threads: one run), the rounds above go through the tile, and
+// the top round stays in registers, where the scale n^-1 g^i is applied.
+// Each coset's forward runs top-down from those registers: the top round
+// (powers of the coset prefix brev(k); none for k = 0), the rounds below
+// through the tile, and the bottom round is stored straight from registers.
+// Against top_body this saves the tile's fill, the top_store round trip, two
+// barriers per coset and, with a short round, its two shared-memory round
+// trips per direction.  The tile region a CTA reads is the one it writes (the
+// intermediate T may be coset block 2^b - 1), and every thread loads its
+// values before the first barrier of the column group.
+template <int K, int C>
+__device__ __forceinline__ void top_body_direct(const LdeTopParams &p, uint32_t bx, uint32_t by, uint64_t *smem) {
+  constexpr int W = 1 << K;
+  constexpr int R = K % 4, NF = K / 4;
+  constexpr int NB = R ? NF : NF - 1;   // full rounds below the top round
+  constexpr int TB = R ? K - R : K - 4; // the top round's bits [TB, K)
+  constexpr int TV = K - TB;
+  constexpr int NV = 1 << TV, NG = 16 / NV;
+  const uint32_t G = 1u << p.log_g;
+  const uint32_t TILE = G * W * C;
+  const uint32_t T = TILE / 16;
+  uint64_t *const tile = smem;
+  uint64_t *pw_inv = smem + top_tables_offset(TILE, 1);
+  uint64_t *pw_fwd = pw_inv + PowWords<K>::words;
+  constexpr uint32_t PW = PowWords<K>::words;
+  const uint32_t tid = threadIdx.x;
+
+  const uint64_t base_off = (uint64_t)bx << LogC<C>::v;
+  const uint32_t col_begin = by * p.cols_per_cta;
+  const uint32_t col_end = min(p.num_cols, col_begin + p.cols_per_cta);
+  const uint32_t nb = 1u << p.log_blowup;
+  if (p.inv_table)
+    copy_table<K, false>(pw_inv, p.inv_table, tid, T);
+  else
+    fill_powers<K, 0, 1>(pw_inv, p.tabs, 1, 0, tid, T);
+  if (p.fwd_mode == TOP_TABLES_RESIDENT) {
+    for (uint32_t k = 0; k < nb; k++) {
+      if (p.fwd_tables)
+        copy_table<K, false>(pw_fwd + k * PW, p.fwd_tables + k * PW, tid, T);
+      else
+        fill_powers<K, 0, 1>(pw_fwd + k * PW, p.tabs, 0, brev_bits(k, p.log_blowup), tid, T,
+                             (k + 1) * PowWords<K>::tasks);
+    }
+  } else if (p.fwd_mode == TOP_TABLES_PREFETCH) {
+    copy_table<K, true>(pw_fwd, p.fwd_tables, tid, T); // coset 0 of the first column
+    cp_async_commit();
+  }
+  uint32_t step = 0; // cosets done so far: PREFETCH keeps step's table in slot step & 1
+  const uint64_t inv_n = p.tabs.inv_pow2[p.log_n];
+
+  // the thread's bottom-round group: window positions w0 + j, low position
+  // base_off + lc, column c0 + g0 of each column group
+  uint32_t w0;
+  const uint32_t eb0 = gbase16<K, C>(tid, 0, w0);
+  const uint32_t lc = tid % C, g0 = (tid / C) >> (K - 4);
+
+  // scale n^-1 g^i of the top round's registers: register q NV + j holds
+  // window position w_q + (j << TB) (group q = tid + T q of that round)
+  auto scale_factors = [&](auto &&use) {
+    const uint64_t g_step = g_power(p.tabs, 0, 1u << (p.lb + TB));
+    if constexpr (R > 0) {
+#pragma unroll
+      for (int q = 0; q < NG; q++) {
+        uint32_t w;
+        group_base<K, C, TB, TV>(tid + T * (uint32_t)q, w);
+        uint64_t s = gl::mul(inv_n, g_power(p.tabs, 0, (uint32_t)base_off + lc + (w << p.lb)));
+#pragma unroll
+        for (int j = 0; j < NV; j++) {
+          use(q * NV + j, s);
+          if (j + 1 < NV) s = gl::mul(s, g_step);
+        }
+      }
+    } else {
+      uint32_t w;
+      gbase16<K, C>(tid, TB, w);
+      uint64_t s = gl::mul(inv_n, g_power(p.tabs, 0, (uint32_t)base_off + lc + (w << p.lb)));
+#pragma unroll
+      for (int j = 0; j < 16; j++) {
+        use(j, s);
+        if (j + 1 < 16) s = gl::mul(s, g_step);
+      }
+    }
+  };
+  uint64_t *const scale_tab = p.scale_off ? smem + p.scale_off : nullptr;
+  if (scale_tab) scale_factors([&](int j, uint64_t s) { scale_tab[j * T + tid] = s; });
+  __syncthreads(); // the tables are complete before the first round reads them
+
+  for (uint32_t c0 = col_begin; c0 < col_end; c0 += G) {
+    const uint32_t col = c0 + g0;
+    const bool live = col < col_end;
+    uint64_t coef[16];
+    {
+      // inverse, bottom round: straight from global memory
+      uint64_t x[16];
+      if (live) {
+        const uint64_t *src = p.in + (uint64_t)col * p.stride_in + base_off + lc;
+#pragma unroll
+        for (int j = 0; j < 16; j++) x[j] = __ldcg(src + ((uint64_t)(w0 + (uint32_t)j) << p.lb));
+      } else {
+#pragma unroll
+        for (int j = 0; j < 16; j++) x[j] = 0;
+      }
+      if constexpr (NB == 0) {
+        net16<K, true, true>(x, pw_inv, w0, 0, false); // the bottom round is the top round: s = 1
+#pragma unroll
+        for (int j = 0; j < 16; j++) coef[j] = x[j];
+      } else {
+        net16<K, true, true>(x, pw_inv, w0, 0, true);
+        uint32_t a[16];
+        slots16(eb0, (uint32_t)C, a);
+        __syncthreads(); // the previous column group's last round has read the tile
+#pragma unroll
+        for (int j = 0; j < 16; j++) tile[a[j]] = x[j];
+        __syncthreads();
+        full_rounds<K, C, true, true>(tile, pw_inv, 4, 4, NB - 1, tid);
+        if constexpr (R > 0) {
+          load_groups<K, C, TB, TV>(tile, coef, tid, T);
+          top_round_groups<true, true, TV>(coef, pw_inv, false);
+        } else {
+          uint32_t w;
+          const uint32_t eb = gbase16<K, C>(tid, TB, w);
+          slots16(eb, (uint32_t)C << TB, a);
+#pragma unroll
+          for (int j = 0; j < 16; j++) coef[j] = tile[a[j]];
+          net16<K, true, true>(coef, pw_inv, w, TB, false);
+        }
+      }
+    }
+    if (scale_tab) {
+#pragma unroll
+      for (int j = 0; j < 16; j++) coef[j] = gl::mul_chain(coef[j], scale_tab[j * T + tid]);
+    } else {
+      scale_factors([&](int j, uint64_t s) { coef[j] = gl::mul(coef[j], s); });
+    }
+
+    for (uint32_t k = 0; k < nb; k++) {
+      __syncthreads(); // the previous round has read the tile and the powers
+      const uint64_t *pwk = pw_fwd;
+      if (p.fwd_mode == TOP_TABLES_RESIDENT) {
+        pwk = pw_fwd + k * PW;
+      } else if (p.fwd_mode == TOP_TABLES_PREFETCH) {
+        // the slot of the previous step is free: start the next step's copy,
+        // then wait for this step's (all but the newest group)
+        pwk = pw_fwd + (step & 1) * PW;
+        const bool more = k + 1 < nb || c0 + G < col_end;
+        if (more) copy_table<K, true>(pw_fwd + ((step + 1) & 1) * PW, p.fwd_tables + ((k + 1) % nb) * PW, tid, T);
+        cp_async_commit();
+        cp_async_wait<1>();
+        __syncthreads();
+      } else {
+        fill_powers<K, 0, 1>(pw_fwd, p.tabs, 0, brev_bits(k, p.log_blowup), tid, T);
+        __syncthreads();
+      }
+      step++;
+      uint64_t x[16];
+#pragma unroll
+      for (int j = 0; j < 16; j++) x[j] = coef[j];
+      if constexpr (NB == 0) {
+        net16<K, false, false>(x, pwk, w0, 0, k != 0);
+      } else {
+        if constexpr (R > 0) {
+          top_round_groups<false, false, TV>(x, pwk, k != 0);
+          store_groups<K, C, TB, TV>(tile, x, tid, T);
+        } else {
+          uint32_t w;
+          const uint32_t eb = gbase16<K, C>(tid, TB, w);
+          net16<K, false, false>(x, pwk, w, TB, k != 0);
+          uint32_t a[16];
+          slots16(eb, (uint32_t)C << TB, a);
+#pragma unroll
+          for (int j = 0; j < 16; j++) tile[a[j]] = x[j];
+        }
+        __syncthreads();
+        full_rounds<K, C, false, false>(tile, pwk, 4 * (NB - 1), -4, NB - 1, tid);
+        uint32_t a[16];
+        slots16(eb0, (uint32_t)C, a);
+#pragma unroll
+        for (int j = 0; j < 16; j++) x[j] = tile[a[j]];
+        net16<K, false, false>(x, pwk, w0, 0, true);
+      }
+      // forward, bottom round: straight to global memory
+      if (live) {
+        uint64_t *dst = p.out + (uint64_t)k * p.coset_stride + (uint64_t)col * p.stride_out + base_off + lc;
+#pragma unroll
+        for (int j = 0; j < 16; j++)
+          __stcg(dst + ((uint64_t)(w0 + (uint32_t)j) << p.lb), p.canon_out ? gl::canon(x[j]) : x[j]);
+      }
+    }
+  }
+  cp_async_wait<0>(); // nothing in flight past the body
+}
+
 // One CTA's work of the top-window kernel: tile position bx (run of low
 // positions), column chunk by.  blockDim.x == 2^log_g * 2^K * C / 16.
 template <int K, int C>
 __device__ __forceinline__ void top_body(const LdeTopParams &p, uint32_t bx, uint32_t by, uint64_t *smem) {
+  if constexpr (top_direct(K, C)) {
+    top_body_direct<K, C>(p, bx, by, smem);
+    return;
+  }
   constexpr int W = 1 << K;
   constexpr int R = K % 4, NF = K / 4;
   const uint32_t G = 1u << p.log_g;
@@ -181,11 +402,13 @@ __device__ __forceinline__ void top_body(const LdeTopParams &p, uint32_t bx, uin
     }
   };
   uint64_t *const scale_tab = (NF > 0 && p.scale_off) ? smem + p.scale_off : nullptr;
-  if (scale_tab) {
-    // each thread reads back only its own factors: no barrier needed
-    uint32_t w;
-    gbase16<K, C>(tid, K - 4, w);
-    scale_factors(w, [&](int j, uint64_t s) { scale_tab[j * T + tid] = s; });
+  if constexpr (NF > 0) {
+    if (scale_tab) {
+      // each thread reads back only its own factors: no barrier needed
+      uint32_t w;
+      gbase16<K, C>(tid, K - 4, w);
+      scale_factors(w, [&](int j, uint64_t s) { scale_tab[j * T + tid] = s; });
+    }
   }
 
   // the tile of column group c by loads and stores

@@ -46,6 +46,7 @@ struct DeviceCtx {
   bool live = false;
   uint64_t *block = nullptr;
   uint64_t *top_pw = nullptr; // precomputed top-window power tables
+  uint64_t *top_pw_st = nullptr; // the same for the short-round-on-top partition
   DevTables tabs{};
   int sms = 0;
 };
@@ -122,8 +123,8 @@ int sm_count() {
 size_t top_pw_base(int K) { return (size_t)(K - 1) * (1u << (TOP_PW_LOG + 1)) - ((1u << K) - 2); }
 size_t top_pw_words() { return top_pw_base(MAX_TOP_K + 1); }
 
-// One block per table t of window size K.
-template <int K> __global__ void top_pw_fill_kernel(const DevTables tabs, uint64_t *base) {
+// One block per table t of window size K, rounds of partition PART.
+template <int K, int PART> __global__ void top_pw_fill_kernel(const DevTables tabs, uint64_t *base) {
   const uint32_t t = blockIdx.x;
   uint32_t inv = 1, H = 0;
   if (t > 0) {
@@ -131,13 +132,13 @@ template <int K> __global__ void top_pw_fill_kernel(const DevTables tabs, uint64
     inv = 0;
     H = brev_bits(k, b);
   }
-  fill_powers<K>(base + (size_t)t * (1u << K), tabs, inv, H, threadIdx.x, blockDim.x);
+  fill_powers<K, 0, PART>(base + (size_t)t * (1u << K), tabs, inv, H, threadIdx.x, blockDim.x);
 }
 
-template <int K> cudaError_t top_pw_fill(const DevTables &tabs, uint64_t *all) {
+template <int K, int PART> cudaError_t top_pw_fill(const DevTables &tabs, uint64_t *all) {
   const uint32_t tables = (1u << (TOP_PW_LOG + 1 - K)) - 1;
-  top_pw_fill_kernel<K><<<tables, 256>>>(tabs, all + top_pw_base(K));
-  if constexpr (K < MAX_TOP_K) return top_pw_fill<K + 1>(tabs, all);
+  top_pw_fill_kernel<K, PART><<<tables, 256>>>(tabs, all + top_pw_base(K));
+  if constexpr (K < MAX_TOP_K) return top_pw_fill<K + 1, PART>(tabs, all);
   return cudaGetLastError();
 }
 
@@ -174,12 +175,15 @@ cudaError_t context_create_current() {
   uint64_t acc = 1;
   for (int k = 0; k <= TW_LOG; k++, acc = hostf::mul(acc, two_inv)) c.tabs.inv_pow2[k] = acc;
   e = cudaMalloc(&c.top_pw, top_pw_words() * sizeof(uint64_t));
-  if (e == cudaSuccess) e = top_pw_fill<1>(c.tabs, c.top_pw);
+  if (e == cudaSuccess) e = cudaMalloc(&c.top_pw_st, top_pw_words() * sizeof(uint64_t));
+  if (e == cudaSuccess) e = top_pw_fill<1, 0>(c.tabs, c.top_pw);
+  if (e == cudaSuccess) e = top_pw_fill<1, 1>(c.tabs, c.top_pw_st);
   if (e == cudaSuccess) e = cudaDeviceSynchronize();
   if (e != cudaSuccess) {
     cudaFree(c.block);
     cudaFree(c.top_pw);
-    c.block = c.top_pw = nullptr;
+    cudaFree(c.top_pw_st);
+    c.block = c.top_pw = c.top_pw_st = nullptr;
     return e;
   }
   cudaDeviceGetAttribute(&c.sms, cudaDevAttrMultiProcessorCount, d);
@@ -187,10 +191,10 @@ cudaError_t context_create_current() {
   return cudaSuccess;
 }
 
-const uint64_t *top_power_tables(uint32_t K, uint32_t log_blowup, bool inverse) {
+const uint64_t *top_power_tables(uint32_t K, uint32_t log_blowup, bool inverse, bool short_top) {
   const int d = current_device();
   if (d < 0 || d >= MAX_DEVICES || !g_ctx[d].live || K < 1 || K > (uint32_t)MAX_TOP_K) return nullptr;
-  const uint64_t *base = g_ctx[d].top_pw + top_pw_base((int)K);
+  const uint64_t *base = (short_top ? g_ctx[d].top_pw_st : g_ctx[d].top_pw) + top_pw_base((int)K);
   if (inverse) return base;
   if (log_blowup < 1 || K + log_blowup > (uint32_t)TOP_PW_LOG) return nullptr;
   return base + ((size_t)(1u << log_blowup) - 1) * (1u << K);
@@ -205,8 +209,10 @@ cudaError_t context_destroy_current() {
   c.live = false;
   cudaError_t e = cudaFree(c.block);
   const cudaError_t e2 = cudaFree(c.top_pw);
+  const cudaError_t e3 = cudaFree(c.top_pw_st);
   if (e == cudaSuccess) e = e2;
-  c.block = c.top_pw = nullptr;
+  if (e == cudaSuccess) e = e3;
+  c.block = c.top_pw = c.top_pw_st = nullptr;
   return e;
 }
 

@@ -57,9 +57,12 @@ const DevTables *device_tables();
 // Power tables (ntt_pass.cuh) of top windows, precomputed per device: for each
 // K <= 12 the inverse table of H = 0, and for each log_blowup b with
 // 2^(K + b) <= 2^TOP_PW_LOG the forward tables of the 2^b cosets
-// (H = brev_b(k)), 2^K words each.  nullptr when not precomputed.
+// (H = brev_b(k)), 2^K words each, for the rounds of the pass kernels'
+// partition (short round at the bottom) or, short_top, of the top-window
+// kernel's direct path (short round at the top).  nullptr when not
+// precomputed.
 constexpr int TOP_PW_LOG = 15;
-const uint64_t *top_power_tables(uint32_t K, uint32_t log_blowup, bool inverse);
+const uint64_t *top_power_tables(uint32_t K, uint32_t log_blowup, bool inverse, bool short_top = false);
 int current_device();
 int sm_count();
 

@@ -238,6 +238,26 @@ template <int K, bool DIF, bool RAGGED_FIRST, int RI> struct RoundShape {
   static constexpr int NR = (K + 3) / 4;
 };
 
+// The other partition of a window, used by the top-window kernel's direct
+// path (lde.cuh): the short round on the window's top bits [K - R, K), full
+// rounds below it down to bit 0.  Rounds are listed top-down (RI = 0 is the
+// top one); with R = 0 it is RoundShape's DIT partition.
+template <int K, int RI> struct ShortTopShape {
+  static constexpr int R = K % 4;
+  static constexpr int V = (R && RI == 0) ? R : 4;
+  static constexpr int B = R ? (RI == 0 ? K - R : K - R - 4 * RI) : K - 4 - 4 * RI;
+  static constexpr int NR = K / 4 + (R ? 1 : 0);
+};
+
+// Round RI of partition PART (0: RoundShape's DIT partition, short round at
+// the bottom; 1: ShortTopShape).
+template <int K, int RI, int PART> struct PartShape {
+  using type = RoundShape<K, false, false, RI>;
+};
+template <int K, int RI> struct PartShape<K, RI, 1> {
+  using type = ShortTopShape<K, RI>;
+};
+
 // Words of a tile position's power table, and its fill tasks (R_local values
 // over all rounds).
 template <int K> struct PowWords {
@@ -264,28 +284,33 @@ __device__ __forceinline__ void fill_round_powers(uint64_t *pw, const DevTables 
 }
 
 // The power table of tile position H (window bits above the window, group
-// prefix included) for the forward (inv = 0) or inverse (inv = 1) twiddles.
-template <int K, int RI = 0>
+// prefix included) for the forward (inv = 0) or inverse (inv = 1) twiddles,
+// for the rounds of partition PART (PartShape).  The layout rule (a round's
+// entries after the NR - 1 of the rounds above it) holds for either.
+template <int K, int RI = 0, int PART = 0>
 __device__ __forceinline__ void fill_powers(uint64_t *pw, const DevTables &tabs, uint32_t inv, uint32_t H,
                                             uint32_t tid, uint32_t nthreads, uint32_t first = 0) {
-  using S = RoundShape<K, false, false, RI>;
+  using S = typename PartShape<K, RI, PART>::type;
   if constexpr (RI < S::NR) {
     fill_round_powers<K, S::B, S::V>(pw, tabs, inv, H, first % nthreads, tid, nthreads);
-    fill_powers<K, RI + 1>(pw, tabs, inv, H, tid, nthreads, first + (1u << (K - S::B - S::V)));
+    fill_powers<K, RI + 1, PART>(pw, tabs, inv, H, tid, nthreads, first + (1u << (K - S::B - S::V)));
   }
 }
 
 // Butterflies by the constant twiddle 2^E (E < 192).  DIT: the product is
 // reduced to [0, p), so the sum and difference need one correction each;
-// with E = 0 the same holds when b is known canonical (BCAN).
+// with E = 0 b itself is reduced first unless it is known canonical (BCAN):
+// 6 + 8 instructions against 16 for the add and subtract of two arbitrary
+// operands.
 template <int E, bool BCAN = false> __device__ __forceinline__ void cdit(uint64_t &a, uint64_t &b) {
   const uint64_t a0 = a;
   if constexpr (E == 0 && BCAN) {
     a = gl::add_bc(a0, b);
     b = gl::sub_bc(a0, b);
   } else if constexpr (E == 0) {
-    a = gl::add(a0, b);
-    b = gl::sub(a0, b);
+    const uint64_t m = gl::canon(b);
+    a = gl::add_bc(a0, m);
+    b = gl::sub_bc(a0, m);
   } else if constexpr (E < 96) {
     const uint64_t m = gl::mul_pow2<E, true>(b);
     a = gl::add_bc(a0, m);
